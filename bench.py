@@ -1,0 +1,439 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Gale-Shapley solver (one JSON line on rank 0).
+
+Workload: one stable-marriage instance, n = 30000, both preference sides
+independent uniform random permutations (seed 2), int32 -- two 3.6 GB lists
+plus the rank matrix, resident in HBM.  A step is one full solve of that
+instance (precheck, rank inversion, proposals, tail, matching) through the C
+ABI with device pointers.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--gpus N under torchrun runs N replicas (one per GPU, no collective on the
+data path: a single instance does not shard).  --impl reference times the
+reference's own multithreaded CPU engine (Mw-Par-Cpu) on the host cores on
+the same instance, on rank 0 only.
+
+Timing: W untimed warm-up solves, then K solves, each timed on the device
+with the library's CUDA events on its own stream; the 7.2 GB inputs exceed
+the 126 MB L2 and a 256 MB buffer is written before every timed solve
+anyway.  The e2e number times smp_b200_solve with pinned host buffers (both
+lists copied in, the matching copied out) by the host clock around the
+synchronous call.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "instances/s batched vs plain per-instance launches; n=30k solve ms; p99 latency"
+N_DEFAULT = 30000
+SEED = 2
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+TRAFFIC_FILE = ROOT / "profiles" / "roofline_traffic.txt"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--kind", type=int, default=0, help="workload kind (0 uniform, 1 congested, 2 correlated)")
+    ap.add_argument("--param", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(args) -> dict:
+    kinds = {0: "uniform random permutations", 1: "congested (men share one row, women uniform)",
+             2: f"correlated (sigma={args.param / 1e4})"}
+    return {
+        "workload": f"single SMP instance n={args.n}, {kinds.get(args.kind, args.kind)}, seed {SEED}, int32 "
+                    f"(two {args.n * args.n * 4 / 1e9:.1f} GB preference lists + rank matrix resident in HBM)",
+        "n": args.n,
+        "kind": args.kind,
+        "seed": SEED,
+        "l2": "inputs (2 x n^2 x 4 B) exceed the 126 MB L2; a 256 MB buffer is written before each timed solve",
+        "parallelism": "replicas" if args.gpus > 1 else "single GPU",
+    }
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local_rank))
+            self.pg = dist
+
+    def _host_only(self, rank: int) -> "Dist":
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = rank
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        return self
+
+    def barrier(self):
+        if self.pg:
+            import torch
+
+            t = torch.ones(1, device=f"cuda:{self.local_rank}")
+            self.pg.all_reduce(t)
+            torch.cuda.synchronize()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local_rank}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local_rank}")
+        self.pg.all_reduce(t)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={CLOCK_FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        loaded = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    try:
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_launch(kernel: str, n: int) -> float | None:
+    """DRAM bytes per launch of `kernel` at size n from the committed ncu
+    summary (lines `kernel=<name> n=<n> dram_bytes=<bytes>`), else None."""
+    try:
+        for line in TRAFFIC_FILE.read_text().splitlines():
+            f = dict(kv.split("=", 1) for kv in line.split() if "=" in kv)
+            if f.get("kernel") == kernel and int(f.get("n", -1)) == n:
+                return float(f["dram_bytes"])
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def run_b200(args, dist: Dist) -> dict | None:
+    import numpy as np
+    import torch
+
+    import pactae_b200 as pb
+
+    dev = dist.local_rank
+    torch.cuda.set_device(dev)
+    n = args.n
+    ctx = pb.Context(device=dev)
+    pm, pw = ctx.generate(args.kind, n, seed=SEED, param=args.param)
+    match = torch.empty(n, dtype=torch.int32, device=f"cuda:{dev}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+
+    def one():
+        flush.random_(0, 255)  # evicts L2 (untimed: the library's events bracket the solve only)
+        torch.cuda.synchronize()
+        _, st = ctx.solve(pm, pw, out=match)
+        return st
+
+    for _ in range(args.warmup):
+        one()
+    dist.barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    t_wall0 = time.perf_counter()
+    steps = [one() for _ in range(args.steps)]
+    t_wall = time.perf_counter() - t_wall0
+    dist.barrier()
+    local_ms = sum(s["total_ms"] for s in steps)
+    total_ms = dist.max(local_ms)  # max over ranks of the device time of K solves
+
+    # parity of the timed result (cheap: against the proposals the fixture records)
+    st0 = steps[-1]
+    launches = int(sum(s["kernel_launches"] for s in steps))
+
+    # e2e through the C ABI with pinned host buffers
+    e2e = None
+    h_pm = h_pw = None
+    if not args.no_e2e:
+        h_pm_t = torch.empty((n, n), dtype=torch.int32, pin_memory=True)
+        h_pw_t = torch.empty((n, n), dtype=torch.int32, pin_memory=True)
+        h_pm_t.copy_(pm)
+        h_pw_t.copy_(pw)
+        h_match = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        h_pm, h_pw, hm = h_pm_t.numpy(), h_pw_t.numpy(), h_match.numpy()
+        del pm, pw
+        torch.cuda.empty_cache()
+        for _ in range(max(1, args.warmup)):
+            ctx.solve(h_pm, h_pw, out=hm)
+        dist.barrier()
+        e2e_times = []
+        for _ in range(args.steps):
+            flush.random_(0, 255)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.solve(h_pm, h_pw, out=hm)
+            e2e_times.append((time.perf_counter() - t0) * 1e3)
+        e2e_total = dist.max(sum(e2e_times))
+        assert np.array_equal(hm, match.cpu().numpy()), "e2e matching differs from the device-input solve"
+        e2e = {"value": e2e_total / (args.steps * dist.world), "unit": "ms",
+               "h2d_bytes_per_step": 2 * n * n * 4, "d2h_bytes_per_step": n * 4,
+               "per_rank_ms_per_solve": e2e_total / args.steps}
+    clk = clocks.stop()
+
+    result = None
+    if dist.rank == 0:
+        ms_per_step = total_ms / args.steps
+        peak, peak_kind = measured_peak_hbm()
+        # Algorithmic bytes per solve: 8 n^2 (inversion: read pref_w, write
+        # the rank matrix as int32) + 36 per proposal (4 B of the man's list
+        # + one 32 B sector of the rank matrix).
+        P = st0["proposals"]
+        b_solve = 8 * n * n + 36 * P
+        kernels = {
+            "k_invert": {"ms": st0["invert_ms"], "bytes": 8 * n * n},
+            "k_bulk": {"ms": st0["bulk_ms"], "bytes": None},
+            "k_tail": {"ms": st0["tail_ms"], "bytes": None},
+        }
+        for k in kernels.values():
+            k["gbs"] = (k["bytes"] / (k["ms"] * 1e-3) / 1e9) if k["bytes"] and k["ms"] else None
+        dominant = max(kernels, key=lambda k: kernels[k]["ms"] or 0)
+        # roofline of the inversion, the bandwidth-bound kernel
+        inv_ms = statistics.mean(s["invert_ms"] for s in steps)
+        inv_ach = 8 * n * n / (inv_ms * 1e-3) / 1e9
+        solve_ach = b_solve / (ms_per_step * 1e-3) / 1e9
+        roofline = {
+            "kernel": "k_invert",
+            "bound": "hbm",
+            "achieved": round(inv_ach, 1),
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": round(inv_ach / peak, 4),
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+            "traffic": traffic_per_launch("k_invert", n),
+            "algorithmic_bytes_per_launch": 8 * n * n,
+            "launch_ms": round(inv_ms, 4),
+            "dominant_kernel_by_time": dominant,
+            "solve": {"bytes": b_solve, "ms": round(ms_per_step, 4), "achieved": round(solve_ach, 1),
+                      "frac": round(solve_ach / peak, 4),
+                      "formula": "8 n^2 + 36 P over the whole solve time"},
+            "kernels": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in v.items()}
+                        for k, v in kernels.items()},
+        }
+        result = {
+            "metric": METRIC,
+            "value": round(total_ms / (args.steps * dist.world), 4),
+            "unit": "ms",
+            "n_gpus": dist.world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "int32",
+            "data": "synthetic (seeded Philox generator, same instance the reference fixtures were solved on)",
+            "config": workload_config(args),
+            "solves_per_s": round(args.steps * dist.world / (total_ms * 1e-3), 2),
+            "proposals": P,
+            "tail_men": st0["tail_men"],
+            "phase_ms": {k: round(st0[k], 4) for k in ("precheck_ms", "init_ms", "core_ms", "post_ms",
+                                                         "invert_ms", "bulk_ms", "tail_ms")},
+            "wall_s_timed_loop": round(t_wall, 3),
+            "roofline": roofline,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+    # CPU baseline: the reference's Mw-Par-Cpu on the same instance, rank 0, N = 1
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline and result is not None:
+        result["cpu_baseline"] = cpu_baseline(args, h_pm, h_pw, match.cpu().numpy(), ctx)
+    ctx.close()
+    return result
+
+
+def cpu_baseline(args, h_pm, h_pw, gpu_match, ctx) -> dict:
+    import numpy as np
+
+    import oracle
+
+    n = args.n
+    if h_pm is None:
+        h_pm, h_pw = oracle.generate(args.kind, n, SEED, 0, args.param)
+    if oracle.ref_available():
+        eng = 3  # Mw-Par-Cpu, min(nproc, 96) threads
+        prob = oracle.RefProblem(h_pm, h_pw)
+        match, ms = prob.solve(eng)
+        prob.close()
+        assert np.array_equal(match, gpu_match), "reference CPU matching differs from the GPU's"
+        return {"value": round(sum(ms), 3), "unit": "ms", "cores": oracle.ref_threads(), "kind": "reference",
+                "sample": f"1 solve of the same n={n} instance by the reference's Mw-Par-Cpu "
+                          f"(smp_engine_mw_2.cu), engine-reported precheck+init+core",
+                "phases_ms": [round(x, 3) for x in ms]}
+    t0 = time.perf_counter()
+    match, _ = oracle.gs_seq(h_pm, h_pw)
+    dt = (time.perf_counter() - t0) * 1e3
+    assert np.array_equal(match, gpu_match)
+    return {"value": round(dt, 3), "unit": "ms", "cores": 1, "kind": "port",
+            "sample": f"1 solve of the same n={n} instance by the oracle's sequential Gale-Shapley"}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CPU engine on the host cores
+# ---------------------------------------------------------------------------
+def run_reference(args, dist: Dist) -> dict | None:
+    if dist.rank != 0:
+        return None
+    import oracle
+
+    if not oracle.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libsmpref.so (the reference's CPU engines) not built"}
+    n = args.n
+    pm, pw = oracle.generate(args.kind, n, SEED, 0, args.param)
+    prob = oracle.RefProblem(pm, pw)
+    del pm, pw
+    eng = 3  # Mw-Par-Cpu
+    for _ in range(args.warmup):
+        prob.solve(eng)
+    times = []
+    for _ in range(args.steps):
+        _, ms = prob.solve(eng)
+        times.append(sum(ms))
+    prob.close()
+    total = sum(times)
+    ms_per_step = total / args.steps
+    threads = oracle.ref_threads()
+    return {
+        "metric": METRIC,
+        "value": round(ms_per_step, 3),
+        "unit": "ms",
+        "n_gpus": dist.world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_per_step, 3),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int32",
+        "data": "synthetic (seeded Philox generator)",
+        "config": workload_config(args),
+        "impl": "reference",
+        "cpu_baseline": {"value": round(ms_per_step, 3), "unit": "ms", "cores": threads, "kind": "reference",
+                         "sample": f"each step one solve of the n={n} instance by the reference's Mw-Par-Cpu "
+                                   f"(smp_engine_mw_2.cu) with {threads} threads, engine-reported "
+                                   "precheck+init+core"},
+        "e2e": {"value": round(ms_per_step, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        # Host-only arm: rank 0 times the reference's CPU engine; other ranks
+        # exit without work and no process group is needed.
+        rank = int(os.environ.get("RANK", "0"))
+        if rank == 0:
+            res = run_reference(args, Dist.__new__(Dist)._host_only(rank))
+            print(json.dumps(res), flush=True)
+        return
+    dist = Dist(args.gpus)
+    try:
+        res = run_b200(args, dist)
+        if res is not None and dist.rank == 0:
+            print(json.dumps(res), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,181 @@
+/*
+ * smp_b200.h -- C ABI of the B200 (sm_100a) Gale-Shapley stable-marriage
+ * solver.
+ *
+ * The reference (victorliu-sq/PACTAE, BambooSMP) has no C or FFI layer; its
+ * public surface is the C++ engine API.  Every entry point below replaces one
+ * piece of that API, cited by file:line within the reference project:
+ *
+ *   smp_b200_create / smp_b200_destroy
+ *       SmpEngineBamboo::SmpEngineBamboo (src/smp/smp_engine_bamboo.cu:6-31),
+ *       which allocates the engine's device arrays, and its destructor
+ *       (include/smp/smp_engine_bamboo.h:19-20).
+ *   smp_b200_stage
+ *       the H2D copy of both preference lists in the engine constructor
+ *       (smp_engine_bamboo.cu:28-29), over the flat row-major lists of
+ *       SmpObj (include/smp/smp.h:8-16).
+ *   smp_b200_precheck    SmpEngineBamboo::IsPerfect (smp_engine_bamboo.h:25-33)
+ *   smp_b200_init        SmpEngineBamboo::InitProc  (smp_engine_bamboo.cu:33-106)
+ *   smp_b200_core        SmpEngineBamboo::CoreProc  (smp_engine_bamboo.cu:108-287),
+ *                        including the host monitor / LAProcedure tail that
+ *                        this library runs on the GPU instead.
+ *   smp_b200_post        SmpEngineBamboo::PostProc  (smp_engine_bamboo.cu:289-306)
+ *   smp_b200_solve       AbsSmpEngine::FindStableMatching
+ *                        (include/smp/smp_engine_abs.h:10-36) in one call.
+ *   smp_b200_stats       the phase timings AbsSmpEngine keeps
+ *                        (smp_engine_abs.h:38-52, :68-70).
+ *   smp_b200_invert      F9RankMatrixInitKernel (src/smp/kernel.cu:672-686) /
+ *                        SmpInitEngine3::InitRankMatrix
+ *                        (include/smp/smp_init_3.h:68-95).
+ *   smp_b200_check       no counterpart (the reference has no stability
+ *                        checker); verifies a Matching as returned by
+ *                        FindStableMatching (include/utils/types.h:44).
+ *   smp_b200_generate    GenerateWorkload (include/utils/generate_workloads_flat.h:250-280),
+ *                        seeded.
+ *   smp_b200_solve_batch many SmpEngineExecutor runs
+ *                        (benchmark/smp_engine_exec.h:6-32) in one launch.
+ *   smp_b200_submit / smp_b200_poll
+ *                        no counterpart (serving loop on top of the solver).
+ *
+ * Conventions.
+ *   - Preference lists are row-major int32 n x n: pref_m[m*n + r] is man m's
+ *     r-th choice, pref_w[w*n + r] is woman w's r-th choice (SmpObj,
+ *     smp.h:14-15).  The result is match[m] = w (Matching, types.h:44).
+ *   - Every call returns an smp_status; none terminates the process (the
+ *     reference's CUDA_CHECK calls std::terminate, include/utils/utils.h:38-47).
+ *   - A context is not thread-safe; use one context per host thread.  All
+ *     calls except smp_b200_submit are synchronous: when they return, the
+ *     GPU work they started has finished.
+ *   - Pointers are host pointers unless SMP_F_DEVICE_PTRS is given, in which
+ *     case they are device pointers on the context's device, ready for use
+ *     (the library runs on its own stream and does not wait on the caller's).
+ */
+#ifndef SMP_B200_H
+#define SMP_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__) || defined(__clang__)
+#define SMP_B200_API __attribute__((visibility("default")))
+#else
+#define SMP_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum smp_status {
+  SMP_OK = 0,
+  SMP_ERR_INVALID_ARG = 1,   /* null pointer, bad flag, n out of range       */
+  SMP_ERR_INVALID_INPUT = 2, /* a preference row is not a permutation       */
+  SMP_ERR_OOM = 3,           /* device or pinned allocation failed          */
+  SMP_ERR_CUDA = 4,          /* a CUDA call failed                          */
+  SMP_ERR_TIMEOUT = 5,       /* a bounded device wait ran out               */
+  SMP_ERR_BUSY = 6,          /* serving: no slot or HBM budget free          */
+  SMP_ERR_NOT_READY = 7,     /* serving: the ticket has not finished         */
+  SMP_ERR_UNSUPPORTED = 8    /* request outside this build's limits          */
+} smp_status;
+
+/* Largest n accepted by any entry point (rank indices, men and positions are
+ * packed into 21-bit fields). */
+#define SMP_B200_MAX_N 1048575
+
+/* Flags (bitwise OR). */
+#define SMP_F_DEVICE_PTRS 0x1u  /* pref_m / pref_w / match are device pointers  */
+#define SMP_F_CHECK 0x2u        /* run the GPU stability checker after solving  */
+#define SMP_F_VALIDATE 0x4u     /* also check every man's row is a permutation   */
+#define SMP_F_NO_PRECHECK 0x8u  /* skip the distinct-first-choices shortcut      */
+
+/* Workload kinds for smp_b200_generate. */
+#define SMP_GEN_UNIFORM 0       /* independent uniform permutations, both sides  */
+#define SMP_GEN_CONGESTED 1     /* all men share one uniform row; women uniform  */
+#define SMP_GEN_CORRELATED 2    /* common score + noise; param = sigma * 1e4     */
+#define SMP_GEN_PERFECT 3       /* reference PERFECT (generate_workloads_flat.h:50-82)  */
+#define SMP_GEN_REF_CONGESTED 4 /* reference CONGESTED (:14-47), both sides      */
+#define SMP_GEN_GROUPED 5       /* reference RANDOM(g) (:85-137); param = g      */
+#define SMP_GEN_SOLO 6          /* reference SOLO (:140-247); n >= 3             */
+
+typedef struct smp_ctx smp_ctx;
+
+typedef struct smp_cfg {
+  int32_t device;          /* CUDA device ordinal                                   */
+  int32_t prefix_k;        /* width of the per-man (woman, rank) prefix; 0 = auto,  */
+                           /* -1 = none                                             */
+  int32_t tail_threshold;  /* free men at which the single-CTA tail takes over;     */
+                           /* 0 = auto, -1 = never                                  */
+  int32_t reserved0;
+  uint64_t hbm_budget;     /* bytes the batch / serving paths may hold resident;    */
+                           /* 0 = 64 GiB                                            */
+  uint64_t reserved1[4];
+} smp_cfg;
+
+typedef struct smp_stats {
+  int64_t proposals;       /* Gale-Shapley proposals (equal for every execution)    */
+  int64_t blocking_pairs;  /* from smp_b200_check / SMP_F_CHECK; -1 if not run     */
+  int64_t tail_proposals;  /* the share of proposals settled by the tail kernel     */
+  int32_t n;
+  int32_t perfect;         /* 1 if the precheck short-circuited the solve          */
+  int32_t tail_men;        /* free men handed to the tail kernel                   */
+  int32_t rank_bytes;      /* bytes per rank-matrix entry (2 or 4)                  */
+  int32_t kernel_launches; /* kernels the call launched                            */
+  int32_t reserved_i;
+  float stage_ms;          /* host->device copy of the inputs                       */
+  float precheck_ms;       /* device time of each phase (CUDA events)              */
+  float init_ms;
+  float core_ms;
+  float post_ms;
+  float check_ms;
+  float total_ms;          /* precheck + init + core + post                        */
+  float invert_ms;         /* rank inversion kernel (part of init)                 */
+  float bulk_ms;           /* all-SM proposal kernel (part of core)                */
+  float tail_ms;           /* single-CTA tail kernel (part of core)                */
+  float reserved[2];
+} smp_stats;
+
+/* Context lifetime.  cfg may be NULL (device 0, defaults). */
+SMP_B200_API int smp_b200_create(smp_ctx **out, const smp_cfg *cfg);
+SMP_B200_API void smp_b200_destroy(smp_ctx *ctx);
+SMP_B200_API const char *smp_b200_strerror(int status);
+SMP_B200_API const char *smp_b200_version(void);
+
+/* Phase API (AbsSmpEngine's template method, one call per phase). */
+SMP_B200_API int smp_b200_stage(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w,
+                   int32_t n, uint32_t flags);
+SMP_B200_API int smp_b200_precheck(smp_ctx *ctx, int32_t *is_perfect);
+SMP_B200_API int smp_b200_init(smp_ctx *ctx);
+SMP_B200_API int smp_b200_core(smp_ctx *ctx);
+SMP_B200_API int smp_b200_post(smp_ctx *ctx, int32_t *match_out, uint32_t flags);
+SMP_B200_API int smp_b200_stats(const smp_ctx *ctx, smp_stats *st);
+
+/* Whole solve: stage + precheck + init + core + post (+ check).  st may be
+ * NULL. */
+SMP_B200_API int smp_b200_solve(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w,
+                   int32_t n, int32_t *match_out, uint32_t flags,
+                   smp_stats *st);
+
+/* Rank matrix rank[w*n + pref_w[w*n + r]] = r as int32. */
+SMP_B200_API int smp_b200_invert(smp_ctx *ctx, const int32_t *pref_w, int32_t n,
+                    int32_t *rank_out, uint32_t flags);
+
+/* Stability checker: counts blocking pairs of match (SMP_ERR_INVALID_INPUT
+ * if match is not a permutation) and the proposal count sum_m (position of
+ * match[m] in m's list + 1). */
+SMP_B200_API int smp_b200_check(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w,
+                   int32_t n, const int32_t *match, uint32_t flags,
+                   int64_t *blocking_pairs, int64_t *proposals);
+
+/* Seeded workload generator.  salt separates instances of a batch; param is
+ * sigma*1e4 (CORRELATED) or the group size (GROUPED).  Writes both lists,
+ * drawn from counter-based Philox4x32-10 streams (pactae_b200/csrc/generate.cu
+ * states the recipe), so the same (kind, n, seed, salt, param) always gives
+ * the same lists. */
+SMP_B200_API int smp_b200_generate(smp_ctx *ctx, int32_t kind, int32_t n, uint64_t seed,
+                      uint32_t salt, int32_t param, int32_t *pref_m,
+                      int32_t *pref_w, uint32_t flags);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SMP_B200_H */

@@ -1,0 +1,314 @@
+"""pactae_b200 -- a B200 (sm_100a) Gale-Shapley stable-marriage solver.
+
+Python mirror of the reference's engine API (victorliu-sq/PACTAE:
+``bamboosmp::SmpObj``, include/smp/smp.h:8-52, and ``AbsSmpEngine``,
+include/smp/smp_engine_abs.h:6-74) over the C ABI in include/smp_b200.h.
+Every solve runs in libsmp_b200.so on the GPU; there is no CPU path.
+
+    >>> import numpy as np, pactae_b200 as pb
+    >>> with pb.Context() as ctx:
+    ...     pm, pw = ctx.generate(pb.SMP_GEN_UNIFORM, 2000, seed=1, device=False)
+    ...     match, stats = ctx.solve(pm, pw)
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+from typing import Any
+
+import numpy as np
+
+from ._lib import (  # noqa: F401  (re-exported constants)
+    ABI_SYMBOLS,
+    LIB_PATH,
+    SMP_B200_MAX_N,
+    SMP_ERR_BUSY,
+    SMP_ERR_CUDA,
+    SMP_ERR_INVALID_ARG,
+    SMP_ERR_INVALID_INPUT,
+    SMP_ERR_NOT_READY,
+    SMP_ERR_OOM,
+    SMP_ERR_TIMEOUT,
+    SMP_ERR_UNSUPPORTED,
+    SMP_F_CHECK,
+    SMP_F_DEVICE_PTRS,
+    SMP_F_NO_PRECHECK,
+    SMP_F_VALIDATE,
+    SMP_GEN_CONGESTED,
+    SMP_GEN_CORRELATED,
+    SMP_GEN_GROUPED,
+    SMP_GEN_PERFECT,
+    SMP_GEN_REF_CONGESTED,
+    SMP_GEN_SOLO,
+    SMP_GEN_UNIFORM,
+    SMP_OK,
+    lib,
+    smp_cfg,
+    smp_stats,
+)
+
+__all__ = ["Context", "SmpError", "SmpObj", "SmpEngineB200", "version"]
+
+
+class SmpError(RuntimeError):
+    """A non-OK smp_status from the library."""
+
+    def __init__(self, status: int, where: str = ""):
+        self.status = status
+        msg = lib.smp_b200_strerror(status).decode()
+        super().__init__(f"{where}: {msg} (status {status})" if where else f"{msg} (status {status})")
+
+
+def _check(status: int, where: str) -> None:
+    if status != SMP_OK:
+        raise SmpError(status, where)
+
+
+def version() -> str:
+    return lib.smp_b200_version().decode()
+
+
+def _is_device_tensor(x: Any) -> bool:
+    return hasattr(x, "is_cuda") and bool(getattr(x, "is_cuda"))
+
+
+def _host_array(x: Any, n: int | None = None, name: str = "array") -> np.ndarray:
+    a = np.ascontiguousarray(x, dtype=np.int32)
+    if n is not None and a.size != n * n:
+        raise ValueError(f"{name} must hold n*n = {n * n} int32 values, got {a.size}")
+    return a
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """One solver context (smp_ctx): a CUDA stream plus grow-only device
+    buffers on one device.  Not thread-safe; use one per thread."""
+
+    def __init__(self, device: int = 0, prefix_k: int = 0, tail_threshold: int = 0, hbm_budget: int = 0):
+        cfg = smp_cfg()
+        cfg.device = device
+        cfg.prefix_k = prefix_k
+        cfg.tail_threshold = tail_threshold
+        cfg.hbm_budget = hbm_budget
+        handle = ctypes.c_void_p()
+        _check(lib.smp_b200_create(ctypes.byref(handle), ctypes.byref(cfg)), "smp_b200_create")
+        self._h = handle
+        self.device = device
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.smp_b200_destroy(self._h)
+        self._h = None
+
+    def __enter__(self) -> "Context":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if self._h is None:
+            raise RuntimeError("context is closed")
+        return self._h
+
+    # -- whole solve ----------------------------------------------------------
+    def solve(self, pref_m: Any, pref_w: Any, n: int | None = None, *, check: bool = False,
+              precheck: bool = True, out: Any = None) -> tuple[Any, dict]:
+        """Man-optimal stable matching of one instance.
+
+        Host inputs (anything numpy can view as int32 n x n) give a numpy
+        result; CUDA tensors (torch, on this context's device) give a CUDA
+        tensor and no host copies.  Returns (match, stats)."""
+        flags = (SMP_F_CHECK if check else 0) | (0 if precheck else SMP_F_NO_PRECHECK)
+        st = smp_stats()
+        if _is_device_tensor(pref_m):
+            import torch
+
+            n = n or int(pref_m.shape[0])
+            for t, name in ((pref_m, "pref_m"), (pref_w, "pref_w")):
+                if t.dtype != torch.int32 or not t.is_contiguous() or t.numel() != n * n:
+                    raise ValueError(f"{name} must be a contiguous int32 CUDA tensor of n*n values")
+            match = out if out is not None else torch.empty(n, dtype=torch.int32, device=pref_m.device)
+            torch.cuda.synchronize(pref_m.device)
+            rc = lib.smp_b200_solve(self.handle, ctypes.c_void_p(pref_m.data_ptr()),
+                                    ctypes.c_void_p(pref_w.data_ptr()), n, ctypes.c_void_p(match.data_ptr()),
+                                    flags | SMP_F_DEVICE_PTRS, ctypes.byref(st))
+            _check(rc, "smp_b200_solve")
+            return match, st.as_dict()
+        pm = _host_array(pref_m)
+        n = n or int(round(np.sqrt(pm.size)))
+        pm = _host_array(pm, n, "pref_m")
+        pw = _host_array(pref_w, n, "pref_w")
+        match = out if out is not None else np.empty(n, dtype=np.int32)
+        rc = lib.smp_b200_solve(self.handle, _ptr(pm), _ptr(pw), n, _ptr(match), flags, ctypes.byref(st))
+        _check(rc, "smp_b200_solve")
+        return match, st.as_dict()
+
+    # -- phases (AbsSmpEngine::FindStableMatching, smp_engine_abs.h:10-36) ---
+    def stage(self, pref_m: np.ndarray, pref_w: np.ndarray, n: int) -> None:
+        self._staged = (_host_array(pref_m, n, "pref_m"), _host_array(pref_w, n, "pref_w"))
+        _check(lib.smp_b200_stage(self.handle, _ptr(self._staged[0]), _ptr(self._staged[1]), n, 0),
+               "smp_b200_stage")
+        self._n = n
+
+    def precheck(self) -> bool:
+        v = ctypes.c_int32(0)
+        _check(lib.smp_b200_precheck(self.handle, ctypes.byref(v)), "smp_b200_precheck")
+        return bool(v.value)
+
+    def init(self) -> None:
+        _check(lib.smp_b200_init(self.handle), "smp_b200_init")
+
+    def core(self) -> None:
+        _check(lib.smp_b200_core(self.handle), "smp_b200_core")
+
+    def post(self) -> np.ndarray:
+        match = np.empty(self._n, dtype=np.int32)
+        _check(lib.smp_b200_post(self.handle, _ptr(match), 0), "smp_b200_post")
+        return match
+
+    def stats(self) -> dict:
+        st = smp_stats()
+        _check(lib.smp_b200_stats(self.handle, ctypes.byref(st)), "smp_b200_stats")
+        return st.as_dict()
+
+    # -- other entry points ---------------------------------------------------
+    def invert(self, pref_w: Any, n: int | None = None) -> Any:
+        if _is_device_tensor(pref_w):
+            import torch
+
+            n = n or int(pref_w.shape[0])
+            rank = torch.empty((n, n), dtype=torch.int32, device=pref_w.device)
+            torch.cuda.synchronize(pref_w.device)
+            _check(lib.smp_b200_invert(self.handle, ctypes.c_void_p(pref_w.data_ptr()), n,
+                                       ctypes.c_void_p(rank.data_ptr()), SMP_F_DEVICE_PTRS), "smp_b200_invert")
+            return rank
+        pw = _host_array(pref_w)
+        n = n or int(round(np.sqrt(pw.size)))
+        pw = _host_array(pw, n, "pref_w")
+        rank = np.empty((n, n), dtype=np.int32)
+        _check(lib.smp_b200_invert(self.handle, _ptr(pw), n, _ptr(rank), 0), "smp_b200_invert")
+        return rank
+
+    def check(self, pref_m: Any, pref_w: Any, match: Any, n: int | None = None) -> tuple[int, int]:
+        """(blocking pairs, proposals) of a matching, computed on the GPU."""
+        bp = ctypes.c_int64(-1)
+        props = ctypes.c_int64(0)
+        if _is_device_tensor(pref_m):
+            import torch
+
+            n = n or int(pref_m.shape[0])
+            torch.cuda.synchronize(pref_m.device)
+            rc = lib.smp_b200_check(self.handle, ctypes.c_void_p(pref_m.data_ptr()),
+                                    ctypes.c_void_p(pref_w.data_ptr()), n, ctypes.c_void_p(match.data_ptr()),
+                                    SMP_F_DEVICE_PTRS, ctypes.byref(bp), ctypes.byref(props))
+        else:
+            pm = _host_array(pref_m)
+            n = n or int(round(np.sqrt(pm.size)))
+            pm = _host_array(pm, n, "pref_m")
+            pw = _host_array(pref_w, n, "pref_w")
+            mt = np.ascontiguousarray(match, dtype=np.int32)
+            if mt.size != n:
+                raise ValueError("match must hold n values")
+            rc = lib.smp_b200_check(self.handle, _ptr(pm), _ptr(pw), n, _ptr(mt), 0, ctypes.byref(bp),
+                                    ctypes.byref(props))
+        _check(rc, "smp_b200_check")
+        return int(bp.value), int(props.value)
+
+    def generate(self, kind: int, n: int, seed: int, salt: int = 0, param: int = 0,
+                 device: bool = True) -> tuple[Any, Any]:
+        """Seeded instance (pref_m, pref_w): CUDA tensors if device, else numpy."""
+        if device:
+            import torch
+
+            dev = torch.device("cuda", self.device)
+            pm = torch.empty((n, n), dtype=torch.int32, device=dev)
+            pw = torch.empty((n, n), dtype=torch.int32, device=dev)
+            torch.cuda.synchronize(dev)
+            _check(lib.smp_b200_generate(self.handle, kind, n, seed, salt, param, ctypes.c_void_p(pm.data_ptr()),
+                                         ctypes.c_void_p(pw.data_ptr()), SMP_F_DEVICE_PTRS), "smp_b200_generate")
+            return pm, pw
+        pm = np.empty((n, n), dtype=np.int32)
+        pw = np.empty((n, n), dtype=np.int32)
+        _check(lib.smp_b200_generate(self.handle, kind, n, seed, salt, param, _ptr(pm), _ptr(pw), 0),
+               "smp_b200_generate")
+        return pm, pw
+
+
+class SmpObj:
+    """Mirror of bamboosmp::SmpObj (include/smp/smp.h:8-52): the two flat
+    row-major preference lists of one instance."""
+
+    def __init__(self, flat_m: Any, flat_w: Any):
+        self.flatten_pref_lists_m = np.ascontiguousarray(flat_m, dtype=np.int32).reshape(-1)
+        self.flatten_pref_lists_w = np.ascontiguousarray(flat_w, dtype=np.int32).reshape(-1)
+
+    @staticmethod
+    def CreateFromFlatLists(flat_m: Any, flat_w: Any, n: int) -> "SmpObj":  # noqa: N802 (reference name)
+        obj = SmpObj(flat_m, flat_w)
+        if obj.flatten_pref_lists_m.size != n * n or obj.flatten_pref_lists_w.size != n * n:
+            raise ValueError("flat lists must hold n*n entries")
+        return obj
+
+
+class SmpEngineB200:
+    """Mirror of an AbsSmpEngine subclass (include/smp/smp_engine_abs.h:6-74)
+    backed by the GPU: FindStableMatching() runs the precheck, init and core
+    phases (each timed with a wall clock, as the reference does) and PostProc,
+    and returns the matching as a list with match[m] = w."""
+
+    def __init__(self, smp: SmpObj, n: int, ctx: Context | None = None):
+        self.smp = smp
+        self.n = int(n)
+        self._own = ctx is None
+        self.ctx = ctx or Context()
+        self.precheck_time_ = 0.0
+        self.init_time_ = 0.0
+        self.core_time_ = 0.0
+        # The reference engines copy the lists to the device in the
+        # constructor, outside the timed phases (smp_engine_bamboo.cu:28-29).
+        self.ctx.stage(smp.flatten_pref_lists_m, smp.flatten_pref_lists_w, self.n)
+
+    def GetEngineName(self) -> str:  # noqa: N802
+        return "B200-GS"
+
+    def FindStableMatching(self) -> list[int]:  # noqa: N802
+        t0 = time.perf_counter()
+        perfect = self.ctx.precheck()
+        t1 = time.perf_counter()
+        self.precheck_time_ = (t1 - t0) * 1e3
+        if not perfect:
+            t0 = time.perf_counter()
+            self.ctx.init()
+            t1 = time.perf_counter()
+            self.init_time_ = (t1 - t0) * 1e3
+            t0 = time.perf_counter()
+            self.ctx.core()
+            t1 = time.perf_counter()
+            self.core_time_ = (t1 - t0) * 1e3
+        return self.ctx.post().tolist()
+
+    def PrintProfilingInfo(self) -> None:  # noqa: N802
+        name = self.GetEngineName()
+        total = self.precheck_time_ + self.init_time_ + self.core_time_
+        print(f"{name} Profiling Info:")
+        print(f"{name} Precheck Time: {self.precheck_time_} ms")
+        print(f"{name} Init Time: {self.init_time_} ms")
+        print(f"{name} Core Time: {self.core_time_} ms")
+        print(f"{name} Total Time: {total} ms")
+        print("=" * 66)
+
+    def close(self) -> None:
+        if self._own:
+            self.ctx.close()

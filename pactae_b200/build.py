@@ -1,0 +1,103 @@
+"""Build recipe for libsmp_b200.so (sm_100a) and the CPU oracle.
+
+``python -m pactae_b200.build`` compiles the CUDA sources in
+``pactae_b200/csrc`` with nvcc straight into ``pactae_b200/libsmp_b200.so``
+(in-tree, so the built library travels with the working tree).  Every source
+is compiled for ``sm_100a`` only.  A rebuild happens only when a source or
+header is newer than the library.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+LIB = PKG / "libsmp_b200.so"
+BUILD_DIR = PKG / "_build"
+
+ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = [
+    "-O3",
+    "-std=c++17",
+    "-lineinfo",
+    "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC",
+    "-Xcompiler", "-fvisibility=hidden",
+    "-Xptxas", "-warn-spills",
+]
+
+SOURCES = ["smp_b200.cu", "generate.cu"]
+
+
+def _nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(cand).exists():
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build libsmp_b200.so")
+    return cand
+
+
+def _inputs() -> list[Path]:
+    files = [p for p in CSRC.iterdir() if p.suffix in (".cu", ".cuh", ".h")]
+    files += [p for p in INCLUDE.iterdir() if p.suffix == ".h"]
+    files.append(Path(__file__))
+    return files
+
+
+def needs_build() -> bool:
+    if not LIB.exists():
+        return True
+    mtime = LIB.stat().st_mtime
+    return any(p.stat().st_mtime > mtime for p in _inputs())
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> Path:
+    """Compile libsmp_b200.so if needed and return its path."""
+    if not force and not needs_build() and not ptxas_info:
+        return LIB
+    nvcc = _nvcc()
+    BUILD_DIR.mkdir(exist_ok=True)
+    objs = []
+    for src in SOURCES:
+        obj = BUILD_DIR / (Path(src).stem + ".o")
+        cmd = [nvcc, *ARCH_FLAGS, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(CSRC / src), "-o", str(obj)]
+        if ptxas_info:
+            cmd += ["-Xptxas", "-v"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        objs.append(str(obj))
+    tmp = LIB.with_suffix(".so.tmp")
+    cmd = [nvcc, *ARCH_FLAGS, "-shared", "-o", str(tmp), *objs, "-Xcompiler", "-fPIC"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def build_oracle(verbose: bool = False) -> None:
+    """Compile the CPU oracle (test infrastructure) and, when the reference
+    sources are present, the reference's own CPU engines."""
+    oracle = ROOT / "oracle"
+    targets = ["all"]
+    ref = Path(os.environ.get("SMP_REFERENCE_DIR", "/root/reference"))
+    if (ref / "src" / "smp" / "smp_engine_gs_1.cu").exists():
+        targets.append("ref")
+    cmd = ["make", "-s", "-C", str(oracle), *targets, f"REF={ref}"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+if __name__ == "__main__":
+    force = "--force" in sys.argv
+    info = "--ptxas-info" in sys.argv
+    print(build(force=force, verbose=True, ptxas_info=info))
+    if "--oracle" in sys.argv:
+        build_oracle(verbose=True)

@@ -1,0 +1,129 @@
+// common.cuh -- device-side building blocks shared by every kernel of the
+// B200 stable-marriage solver: the per-solve control block, the packed bid
+// word, relaxed/acquire-release PTX memory operations and Philox4x32-10.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace smpb200 {
+
+constexpr unsigned kFullMask = 0xFFFFFFFFu;
+
+// Status codes written by kernels; the values equal smp_status.
+constexpr int kStatusOk = 0;
+constexpr int kStatusInvalidInput = 2;
+
+// Per-solve control block in device memory.  Kernels of one solve share it;
+// the host zeroes it (and sets free_count = n, perfect = 1) before the solve.
+struct Control {
+  int32_t status;        // first error a kernel saw (kStatus*), 0 if none
+  int32_t perfect;       // 1 while every first choice seen so far is distinct
+  int32_t next_man;      // bulk kernel: next man that has not proposed yet
+  int32_t free_count;    // women that have not received a proposal yet
+  int32_t tail_count;    // men handed from the bulk kernel to the tail kernel
+  int32_t tail_men;      // men the tail kernel started chains for
+  int32_t bad_value;     // first out-of-range preference value seen
+  int32_t pad0;
+  unsigned long long proposals;  // sum over men of (final position + 1)
+  unsigned long long blocking;   // checker: blocking pairs
+  unsigned long long check_proposals;  // checker: proposals recounted from the matching
+  unsigned long long bulk_proposals;   // proposals settled by k_bulk
+  unsigned long long tail_proposals;   // proposals settled by k_tail
+  unsigned long long pad1;
+};
+
+__device__ __forceinline__ void report(Control *ctrl, int status, int value) {
+  if (atomicCAS(&ctrl->status, 0, status) == 0) ctrl->bad_value = value;
+}
+
+// ---------------------------------------------------------------------------
+// Bid word of a woman in global memory (64 bits):
+//   rank of her current partner (21 bits) << 42 | partner (21) << 21 | the
+//   position of this woman in the partner's list (21).
+// A smaller word means a better partner for her (ranks of one woman are
+// distinct), so atomicMin keeps the best proposal and returns the displaced
+// one together with where that man resumes.  kFree (all ones) means no
+// proposal yet.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kFree = ~0ull;
+constexpr uint32_t kMask21 = (1u << 21) - 1;
+
+__device__ __forceinline__ unsigned long long pack_bid(uint32_t rank, uint32_t man,
+                                                       uint32_t pos) {
+  return (static_cast<unsigned long long>(rank) << 42) |
+         (static_cast<unsigned long long>(man) << 21) | pos;
+}
+__device__ __forceinline__ uint32_t bid_rank(unsigned long long b) {
+  return static_cast<uint32_t>(b >> 42);
+}
+__device__ __forceinline__ uint32_t bid_man(unsigned long long b) {
+  return static_cast<uint32_t>(b >> 21) & kMask21;
+}
+__device__ __forceinline__ uint32_t bid_pos(unsigned long long b) {
+  return static_cast<uint32_t>(b) & kMask21;
+}
+
+// ---------------------------------------------------------------------------
+// Memory operations with explicit PTX semantics.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_relaxed_s32(const int *p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_volatile_s32(const int *p) {
+  return *reinterpret_cast<const volatile int *>(p);
+}
+
+// Shared-memory helpers for the single-CTA tail.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint32_t lds_relaxed_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(smem_addr(p)) : "memory");
+  return v;
+}
+// atomicMin with acquire-release semantics at CTA scope: the release half
+// publishes the proposer's position written just before; the acquire half
+// makes the displaced man's published position visible to this thread.
+__device__ __forceinline__ uint32_t atom_min_acq_rel_shared(uint32_t *p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.cta.shared::cta.min.u32 %0, [%1], %2;"
+               : "=r"(old) : "r"(smem_addr(p)), "r"(v) : "memory");
+  return old;
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), the counter-based
+// generator behind every seeded workload.
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2,
+                                                       uint32_t c3, uint32_t k0, uint32_t k1,
+                                                       uint32_t out[4]) {
+#pragma unroll
+  for (int round = 0; round < 10; ++round) {
+    const uint64_t p0 = static_cast<uint64_t>(0xD2511F53u) * c0;
+    const uint64_t p1 = static_cast<uint64_t>(0xCD9E8D57u) * c2;
+    const uint32_t n0 = static_cast<uint32_t>(p1 >> 32) ^ c1 ^ k0;
+    const uint32_t n2 = static_cast<uint32_t>(p0 >> 32) ^ c3 ^ k1;
+    c1 = static_cast<uint32_t>(p1);
+    c3 = static_cast<uint32_t>(p0);
+    c0 = n0;
+    c2 = n2;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+
+}  // namespace smpb200

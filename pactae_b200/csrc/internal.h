@@ -1,0 +1,114 @@
+// internal.h -- host-side state shared by the translation units of
+// libsmp_b200.so.  Not part of the public ABI (include/smp_b200.h is).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+
+#include "smp_b200.h"
+
+namespace smpb200 {
+
+// Grow-only device allocation.
+struct DeviceBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+
+  int ensure(size_t need) {
+    if (need <= bytes && ptr) return SMP_OK;
+    release();
+    if (need == 0) need = 16;
+    if (cudaMalloc(&ptr, need) != cudaSuccess) {
+      cudaGetLastError();  // clear the sticky-free allocation error
+      ptr = nullptr;
+      bytes = 0;
+      return SMP_ERR_OOM;
+    }
+    bytes = need;
+    return SMP_OK;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <typename T>
+  T *as() const { return static_cast<T *>(ptr); }
+};
+
+// Makes the context's device current for the duration of an entry point and
+// restores the caller's device afterwards.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+struct Control;  // common.cuh
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 148;
+  size_t smem_optin = 0;  // max dynamic shared memory per block
+  int prefix_k_cfg = 0;
+  int tail_threshold_cfg = 0;
+  uint64_t hbm_budget = 64ull << 30;
+  std::string last_error;
+
+  // State of the staged solve.
+  int n = 0;
+  bool staged = false;
+  const int32_t *pref_m = nullptr;  // device pointers the solve reads
+  const int32_t *pref_w = nullptr;
+  int K = 0;               // prefix width (0 = none)
+  int tail_threshold = 0;  // 0 = tail kernel disabled
+  int rank_bytes = 2;
+  bool rank_valid = false;  // d_rank holds the inversion of pref_w
+  bool tail_ran = false;
+  int phase = 0;            // 0 staged, 1 prechecked, 2 inited, 3 cored, 4 posted
+
+  DeviceBuf d_pref_m, d_pref_w, d_rank, d_prefix, d_bid, d_tailq, d_seen, d_ctrl, d_match;
+  DeviceBuf d_husband, d_prank;
+  DeviceBuf gen_keys_a, gen_keys_b, gen_seg, gen_temp, gen_aux;
+  Control *h_ctrl = nullptr;  // pinned host copy of the control block
+  cudaEvent_t ev[10] = {};
+  int launches = 0;  // kernels launched since the last stage / call
+  smp_stats stats = {};
+
+  int fail_cuda(const char *what) {
+    const cudaError_t e = cudaGetLastError();
+    last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return SMP_ERR_CUDA;
+  }
+  int check_launch(const char *what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return SMP_OK;
+    last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return SMP_ERR_CUDA;
+  }
+  int sync(const char *what) {
+    const cudaError_t e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) return SMP_OK;
+    last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return SMP_ERR_CUDA;
+  }
+};
+
+// generate.cu
+int generate_side(Ctx &c, int kind, int side, int n, uint64_t seed, uint32_t salt, int param,
+                  int32_t *out);
+
+}  // namespace smpb200
+
+struct smp_ctx {
+  smpb200::Ctx c;
+};

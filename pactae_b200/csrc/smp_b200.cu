@@ -1,0 +1,671 @@
+// smp_b200.cu -- the C ABI of include/smp_b200.h: context, phases of one
+// solve, the whole-solve call, rank inversion, stability check and the
+// seeded generator.  Host code only orchestrates; the work is in
+// solve_kernels.cuh and generate.cu.
+#include <cstdio>
+#include <cstring>
+
+#include "common.cuh"
+#include "internal.h"
+#include "solve_kernels.cuh"
+
+using namespace smpb200;
+
+namespace {
+
+constexpr int kDefaultPrefixK = 128;
+constexpr int kDefaultTailThreshold = 32;
+constexpr int kU16MaxN = 65535;
+
+inline bool valid_ctx(const smp_ctx *ctx) { return ctx != nullptr && ctx->c.stream != nullptr; }
+
+// Phase-boundary events recorded on the context's stream.
+enum Ev {
+  kEvStageBegin = 0,
+  kEvStageEnd = 1,     // = precheck begin
+  kEvPrecheckEnd = 2,  // = init begin
+  kEvInvertEnd = 3,
+  kEvInitEnd = 4,      // = core begin
+  kEvBulkEnd = 5,
+  kEvCoreEnd = 6,      // = post begin
+  kEvPostEnd = 7,
+  kEvCheckBegin = 8,
+  kEvCheckEnd = 9,
+};
+
+float elapsed(const Ctx &c, int a, int b) {
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, c.ev[a], c.ev[b]) != cudaSuccess) {
+    cudaGetLastError();
+    return 0.f;
+  }
+  return ms;
+}
+
+int rank_bytes_for(int n) { return n <= kU16MaxN ? 2 : 4; }
+
+// Blocks per SM that k_bulk can keep resident.
+template <typename RankT>
+int bulk_grid(const Ctx &c) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bulk<RankT>, 256, 0) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 4;
+  }
+  return c.sm_count * std::max(per_sm, 1);
+}
+
+// --------------------------------------------------------------------------
+// Phase bodies (enqueue only; the public entry points add sync + readback).
+// --------------------------------------------------------------------------
+// SMP_F_VALIDATE: both lists, every row a permutation.
+int enqueue_validate(Ctx &c) {
+  const int n = c.n;
+  const size_t smem = ((static_cast<size_t>(n) + 31) / 32) * 4;
+  if (smem > c.smem_optin) {
+    c.last_error = "validate: n too large for the shared-memory bitmap";
+    return SMP_ERR_UNSUPPORTED;
+  }
+  if (cudaFuncSetAttribute(k_validate_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+      cudaSuccess)
+    return c.fail_cuda("k_validate_rows smem attribute");
+  const int grid = std::min(n, c.sm_count * 4);
+  k_validate_rows<<<grid, 512, smem, c.stream>>>(c.pref_m, n, c.d_ctrl.as<Control>());
+  k_validate_rows<<<grid, 512, smem, c.stream>>>(c.pref_w, n, c.d_ctrl.as<Control>());
+  c.launches += 2;
+  return c.check_launch("k_validate_rows");
+}
+
+int enqueue_precheck(Ctx &c, bool run_precheck) {
+  const int n = c.n;
+  Control init = {};
+  init.perfect = run_precheck ? 1 : 0;
+  init.free_count = n;
+  std::memcpy(c.h_ctrl, &init, sizeof(Control));
+  if (cudaMemcpyAsync(c.d_ctrl.ptr, c.h_ctrl, sizeof(Control), cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+    return c.fail_cuda("control reset");
+  if (run_precheck) {
+    const size_t words = (static_cast<size_t>(n) + 31) / 32;
+    if (cudaMemsetAsync(c.d_seen.ptr, 0, words * 4, c.stream) != cudaSuccess) return c.fail_cuda("seen reset");
+    const int grid = std::min(c.sm_count * 4, (n + 255) / 256);
+    k_precheck<<<grid, 256, 0, c.stream>>>(c.pref_m, n, c.d_seen.as<uint32_t>(), c.d_ctrl.as<Control>());
+    c.launches++;
+    return c.check_launch("k_precheck");
+  }
+  return SMP_OK;
+}
+
+template <typename RankT>
+int enqueue_invert(Ctx &c, const int32_t *pref_w, RankT *rank, int mode) {
+  const int n = c.n;
+  const size_t smem = static_cast<size_t>(n) * sizeof(RankT);
+  const size_t smem_padded = (smem + 15) & ~static_cast<size_t>(15);
+  if (smem_padded <= c.smem_optin) {
+    if (cudaFuncSetAttribute(k_invert<RankT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem_padded)) != cudaSuccess)
+      return c.fail_cuda("k_invert smem attribute");
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_invert<RankT>, 512, smem_padded) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    const int grid = std::min(n, c.sm_count * std::max(per_sm, 1));
+    k_invert<RankT><<<grid, 512, smem_padded, c.stream>>>(pref_w, rank, n, c.d_ctrl.as<Control>(), mode);
+    c.launches++;
+    return c.check_launch("k_invert");
+  }
+  // Rows too long for shared memory (int32 ranks only).
+  int32_t *r32 = reinterpret_cast<int32_t *>(rank);
+  k_invert_global<<<c.sm_count * 8, 256, 0, c.stream>>>(pref_w, r32, n, c.d_ctrl.as<Control>(), mode);
+  c.launches++;
+  int rc = c.check_launch("k_invert_global");
+  if (rc) return rc;
+  k_invert_verify<<<c.sm_count * 8, 256, 0, c.stream>>>(pref_w, r32, n, c.d_ctrl.as<Control>(), mode);
+  c.launches++;
+  return c.check_launch("k_invert_verify");
+}
+
+int enqueue_init(Ctx &c) {
+  const int n = c.n;
+  const size_t nn = static_cast<size_t>(n) * n;
+  c.rank_bytes = rank_bytes_for(n);
+  int rc = c.d_rank.ensure(nn * c.rank_bytes);
+  if (!rc) rc = c.d_bid.ensure(sizeof(unsigned long long) * n);
+  if (rc) return rc;
+  // Prefix width and tail eligibility.
+  c.K = 0;
+  if (c.rank_bytes == 2 && c.prefix_k_cfg >= 0) {
+    const int want = c.prefix_k_cfg > 0 ? c.prefix_k_cfg : kDefaultPrefixK;
+    c.K = std::min(want, n);
+  }
+  if (c.K > 0) {
+    rc = c.d_prefix.ensure(sizeof(uint32_t) * static_cast<size_t>(n) * c.K);
+    if (rc) return rc;
+  }
+  c.tail_threshold = 0;
+  if (c.tail_threshold_cfg >= 0 && n <= kU16MaxN && tail_smem_bytes(n) <= c.smem_optin) {
+    c.tail_threshold = c.tail_threshold_cfg > 0 ? c.tail_threshold_cfg : kDefaultTailThreshold;
+  }
+  // Every woman starts free (SmpEngineBamboo::InitProc fills partner_rank
+  // with n, smp_engine_bamboo.cu:37).
+  if (cudaMemsetAsync(c.d_bid.ptr, 0xFF, sizeof(unsigned long long) * n, c.stream) != cudaSuccess)
+    return c.fail_cuda("bid reset");
+  if (c.rank_bytes == 2) {
+    rc = enqueue_invert<uint16_t>(c, c.pref_w, c.d_rank.as<uint16_t>(), kInvertUnlessPerfect);
+  } else {
+    rc = enqueue_invert<int32_t>(c, c.pref_w, c.d_rank.as<int32_t>(), kInvertUnlessPerfect);
+  }
+  if (rc) return rc;
+  if (cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  c.rank_valid = true;
+  if (c.K > 0) {
+    const size_t total = static_cast<size_t>(n) * c.K;
+    const int grid = static_cast<int>(std::min<size_t>(static_cast<size_t>(c.sm_count) * 16, (total + 255) / 256));
+    k_prefix<<<grid, 256, 0, c.stream>>>(c.pref_m, c.d_rank.as<uint16_t>(), c.d_prefix.as<uint32_t>(), n, c.K,
+                                         c.d_ctrl.as<Control>());
+    c.launches++;
+    rc = c.check_launch("k_prefix");
+  }
+  return rc;
+}
+
+template <typename RankT>
+int enqueue_core_t(Ctx &c) {
+  const int n = c.n;
+  int rc = c.d_tailq.ensure(sizeof(int2) * static_cast<size_t>(n));
+  if (!rc) rc = c.d_match.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (rc) return rc;
+  const RankT *rank = reinterpret_cast<const RankT *>(c.d_rank.ptr);
+  const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
+  k_bulk<RankT><<<bulk_grid<RankT>(c), 256, 0, c.stream>>>(c.pref_m, rank, prefix, c.K,
+                                                           c.d_bid.as<unsigned long long>(), c.d_ctrl.as<Control>(),
+                                                           c.d_tailq.as<int2>(), n, c.tail_threshold);
+  c.launches++;
+  rc = c.check_launch("k_bulk");
+  if (rc) return rc;
+  if (cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  c.tail_ran = false;
+  if (c.tail_threshold > 0) {
+    const size_t smem = tail_smem_bytes(n);
+    if (cudaFuncSetAttribute(k_tail<RankT>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+        cudaSuccess)
+      return c.fail_cuda("k_tail smem attribute");
+    k_tail<RankT><<<1, 1024, smem, c.stream>>>(c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(),
+                                               c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
+                                               c.d_match.as<int32_t>(), n);
+    c.launches++;
+    rc = c.check_launch("k_tail");
+    c.tail_ran = true;
+  }
+  return rc;
+}
+
+int enqueue_core(Ctx &c) { return c.rank_bytes == 2 ? enqueue_core_t<uint16_t>(c) : enqueue_core_t<int32_t>(c); }
+
+int enqueue_post(Ctx &c) {
+  if (c.tail_ran) return SMP_OK;  // the tail kernel already wrote d_match
+  const int n = c.n;
+  int rc = c.d_match.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (rc) return rc;
+  const int grid = std::min(c.sm_count * 4, (n + 255) / 256);
+  k_match<<<grid, 256, 0, c.stream>>>(c.pref_m, c.d_bid.as<unsigned long long>(), c.d_match.as<int32_t>(), n,
+                                      c.d_ctrl.as<Control>());
+  c.launches++;
+  return c.check_launch("k_match");
+}
+
+// Copy d_match out to the caller.
+int copy_match_out(Ctx &c, int32_t *match_out, bool device) {
+  const size_t bytes = sizeof(int32_t) * static_cast<size_t>(c.n);
+  const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (cudaMemcpyAsync(match_out, c.d_match.ptr, bytes, kind, c.stream) != cudaSuccess)
+    return c.fail_cuda("match copy");
+  return SMP_OK;
+}
+
+int read_control(Ctx &c) {
+  if (cudaMemcpyAsync(c.h_ctrl, c.d_ctrl.ptr, sizeof(Control), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess)
+    return c.fail_cuda("control readback");
+  return SMP_OK;
+}
+
+int control_status(Ctx &c) {
+  const int s = c.h_ctrl->status;
+  if (s != 0) {
+    char buf[96];
+    std::snprintf(buf, sizeof(buf), "invalid input detected on the device (value %d)", c.h_ctrl->bad_value);
+    c.last_error = buf;
+  }
+  return s;
+}
+
+// Checker body: needs c.pref_m, c.d_rank valid for c.n.
+template <typename RankT>
+int enqueue_check_t(Ctx &c, const int32_t *match) {
+  const int n = c.n;
+  int rc = c.d_husband.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (!rc) rc = c.d_prank.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (rc) return rc;
+  if (cudaMemsetAsync(c.d_husband.ptr, 0xFF, sizeof(int32_t) * static_cast<size_t>(n), c.stream) != cudaSuccess)
+    return c.fail_cuda("husband reset");
+  const int grid = std::min(c.sm_count * 4, (n + 255) / 256);
+  k_check_husband<<<grid, 256, 0, c.stream>>>(match, c.d_husband.as<int32_t>(), n, c.d_ctrl.as<Control>());
+  k_check_prank<RankT><<<grid, 256, 0, c.stream>>>(c.d_husband.as<int32_t>(), reinterpret_cast<const RankT *>(c.d_rank.ptr),
+                                                  c.d_prank.as<int32_t>(), n, c.d_ctrl.as<Control>());
+  const int sgrid = std::min(c.sm_count * 8, (n * 32 + 255) / 256);
+  k_check_scan<RankT><<<sgrid, 256, 0, c.stream>>>(c.pref_m, reinterpret_cast<const RankT *>(c.d_rank.ptr), match,
+                                                  c.d_prank.as<int32_t>(), n, c.d_ctrl.as<Control>());
+  c.launches += 3;
+  return c.check_launch("k_check");
+}
+
+int enqueue_check(Ctx &c, const int32_t *match) {
+  return c.rank_bytes == 2 ? enqueue_check_t<uint16_t>(c, match) : enqueue_check_t<int32_t>(c, match);
+}
+
+// Bring the inputs onto the device (or adopt device pointers).
+int do_stage(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, uint32_t flags) {
+  if (!pref_m || !pref_w || n <= 0 || n > SMP_B200_MAX_N) {
+    c.last_error = "stage: null list or n out of range";
+    return SMP_ERR_INVALID_ARG;
+  }
+  c.n = n;
+  c.staged = false;
+  c.rank_valid = false;
+  c.phase = 0;
+  c.stats = smp_stats{};
+  c.stats.n = n;
+  c.stats.blocking_pairs = -1;
+  c.launches = 0;
+  int rc = c.d_ctrl.ensure(sizeof(Control));
+  if (!rc) rc = c.d_seen.ensure(((static_cast<size_t>(n) + 31) / 32) * 4);
+  if (rc) return rc;
+  if (cudaEventRecord(c.ev[kEvStageBegin], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  if (flags & SMP_F_DEVICE_PTRS) {
+    c.pref_m = pref_m;
+    c.pref_w = pref_w;
+  } else {
+    const size_t bytes = sizeof(int32_t) * static_cast<size_t>(n) * n;
+    rc = c.d_pref_w.ensure(bytes);
+    if (!rc) rc = c.d_pref_m.ensure(bytes);
+    if (rc) return rc;
+    if (cudaMemcpyAsync(c.d_pref_w.ptr, pref_w, bytes, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+      return c.fail_cuda("pref_w copy");
+    if (cudaMemcpyAsync(c.d_pref_m.ptr, pref_m, bytes, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+      return c.fail_cuda("pref_m copy");
+    c.pref_m = c.d_pref_m.as<int32_t>();
+    c.pref_w = c.d_pref_w.as<int32_t>();
+  }
+  if (cudaEventRecord(c.ev[kEvStageEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  c.staged = true;
+  return SMP_OK;
+}
+
+void fill_stats(Ctx &c, bool timed_phases) {
+  c.stats.proposals = static_cast<int64_t>(c.h_ctrl->proposals);
+  c.stats.tail_proposals = static_cast<int64_t>(c.h_ctrl->tail_proposals);
+  c.stats.perfect = c.h_ctrl->perfect;
+  c.stats.tail_men = c.tail_ran ? c.h_ctrl->tail_men : 0;
+  c.stats.rank_bytes = c.rank_bytes;
+  c.stats.kernel_launches = c.launches;
+  if (timed_phases) {
+    c.stats.stage_ms = elapsed(c, kEvStageBegin, kEvStageEnd);
+    c.stats.precheck_ms = elapsed(c, kEvStageEnd, kEvPrecheckEnd);
+    c.stats.init_ms = elapsed(c, kEvPrecheckEnd, kEvInitEnd);
+    c.stats.core_ms = elapsed(c, kEvInitEnd, kEvCoreEnd);
+    c.stats.post_ms = elapsed(c, kEvCoreEnd, kEvPostEnd);
+    c.stats.total_ms = elapsed(c, kEvStageEnd, kEvPostEnd);
+  }
+  // Kernel-level times exist when the inversion and proposal kernels ran.
+  if (c.phase >= 3 && !c.h_ctrl->perfect) {
+    c.stats.invert_ms = elapsed(c, kEvPrecheckEnd, kEvInvertEnd);
+    c.stats.bulk_ms = elapsed(c, kEvInitEnd, kEvBulkEnd);
+    c.stats.tail_ms = c.tail_ran ? elapsed(c, kEvBulkEnd, kEvCoreEnd) : 0.f;
+  }
+}
+
+}  // namespace
+
+// ===========================================================================
+// Public ABI
+// ===========================================================================
+extern "C" {
+
+const char *smp_b200_version(void) { return "smp_b200 0.1 (sm_100a)"; }
+
+const char *smp_b200_strerror(int status) {
+  switch (status) {
+    case SMP_OK: return "ok";
+    case SMP_ERR_INVALID_ARG: return "invalid argument";
+    case SMP_ERR_INVALID_INPUT: return "invalid input: a preference row is not a permutation of 0..n-1";
+    case SMP_ERR_OOM: return "out of device or pinned memory";
+    case SMP_ERR_CUDA: return "CUDA error";
+    case SMP_ERR_TIMEOUT: return "a bounded device wait timed out";
+    case SMP_ERR_BUSY: return "no slot or HBM budget free";
+    case SMP_ERR_NOT_READY: return "not finished yet";
+    case SMP_ERR_UNSUPPORTED: return "unsupported request";
+    default: return "unknown status";
+  }
+}
+
+int smp_b200_create(smp_ctx **out, const smp_cfg *cfg) {
+  if (!out) return SMP_ERR_INVALID_ARG;
+  *out = nullptr;
+  smp_ctx *ctx = new (std::nothrow) smp_ctx();
+  if (!ctx) return SMP_ERR_OOM;
+  Ctx &c = ctx->c;
+  if (cfg) {
+    c.device = cfg->device;
+    c.prefix_k_cfg = cfg->prefix_k;
+    c.tail_threshold_cfg = cfg->tail_threshold;
+    if (cfg->hbm_budget) c.hbm_budget = cfg->hbm_budget;
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || c.device < 0 || c.device >= count) {
+    cudaGetLastError();
+    delete ctx;
+    return SMP_ERR_CUDA;
+  }
+  DeviceGuard g(c.device);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, c.device) != cudaSuccess) {
+    delete ctx;
+    return SMP_ERR_CUDA;
+  }
+  c.sm_count = prop.multiProcessorCount;
+  c.smem_optin = prop.sharedMemPerBlockOptin;
+  if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return SMP_ERR_CUDA;
+  }
+  for (auto &e : c.ev) {
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      smp_b200_destroy(ctx);
+      return SMP_ERR_CUDA;
+    }
+  }
+  if (cudaMallocHost(reinterpret_cast<void **>(&c.h_ctrl), sizeof(Control)) != cudaSuccess) {
+    cudaGetLastError();
+    smp_b200_destroy(ctx);
+    return SMP_ERR_OOM;
+  }
+  std::memset(c.h_ctrl, 0, sizeof(Control));
+  *out = ctx;
+  return SMP_OK;
+}
+
+void smp_b200_destroy(smp_ctx *ctx) {
+  if (!ctx) return;
+  Ctx &c = ctx->c;
+  {
+    DeviceGuard g(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    for (DeviceBuf *b : {&c.d_pref_m, &c.d_pref_w, &c.d_rank, &c.d_prefix, &c.d_bid, &c.d_tailq, &c.d_seen,
+                         &c.d_ctrl, &c.d_match, &c.d_husband, &c.d_prank, &c.gen_keys_a, &c.gen_keys_b, &c.gen_seg,
+                         &c.gen_temp, &c.gen_aux})
+      b->release();
+    for (auto &e : c.ev)
+      if (e) cudaEventDestroy(e);
+    if (c.h_ctrl) cudaFreeHost(c.h_ctrl);
+    if (c.stream) cudaStreamDestroy(c.stream);
+  }
+  delete ctx;
+}
+
+int smp_b200_stage(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w, int32_t n, uint32_t flags) {
+  if (!valid_ctx(ctx)) return SMP_ERR_INVALID_ARG;
+  Ctx &c = ctx->c;
+  DeviceGuard g(c.device);
+  int rc = do_stage(c, pref_m, pref_w, n, flags);
+  if (rc) return rc;
+  rc = c.sync("stage");
+  if (rc) return rc;
+  c.stats.stage_ms = elapsed(c, kEvStageBegin, kEvStageEnd);
+  return SMP_OK;
+}
+
+int smp_b200_precheck(smp_ctx *ctx, int32_t *is_perfect) {
+  if (!valid_ctx(ctx) || !ctx->c.staged) return SMP_ERR_INVALID_ARG;
+  Ctx &c = ctx->c;
+  DeviceGuard g(c.device);
+  if (cudaEventRecord(c.ev[kEvStageEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  int rc = enqueue_precheck(c, true);
+  if (!rc) rc = read_control(c);
+  if (rc) return rc;
+  if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  rc = c.sync("precheck");
+  if (rc) return rc;
+  c.phase = 1;
+  c.stats.precheck_ms = elapsed(c, kEvStageEnd, kEvPrecheckEnd);
+  if (is_perfect) *is_perfect = c.h_ctrl->perfect;
+  return control_status(c);
+}
+
+int smp_b200_init(smp_ctx *ctx) {
+  if (!valid_ctx(ctx) || ctx->c.phase < 1) return SMP_ERR_INVALID_ARG;
+  Ctx &c = ctx->c;
+  DeviceGuard g(c.device);
+  if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  int rc = enqueue_init(c);
+  if (rc) return rc;
+  if (cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  rc = read_control(c);
+  if (!rc) rc = c.sync("init");
+  if (rc) return rc;
+  c.phase = 2;
+  c.stats.init_ms = elapsed(c, kEvPrecheckEnd, kEvInitEnd);
+  return control_status(c);
+}
+
+int smp_b200_core(smp_ctx *ctx) {
+  if (!valid_ctx(ctx) || ctx->c.phase < 2) return SMP_ERR_INVALID_ARG;
+  Ctx &c = ctx->c;
+  DeviceGuard g(c.device);
+  if (cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  int rc = enqueue_core(c);
+  if (rc) return rc;
+  if (cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  rc = read_control(c);
+  if (!rc) rc = c.sync("core");
+  if (rc) return rc;
+  c.phase = 3;
+  c.stats.core_ms = elapsed(c, kEvInitEnd, kEvCoreEnd);
+  return control_status(c);
+}
+
+int smp_b200_post(smp_ctx *ctx, int32_t *match_out, uint32_t flags) {
+  if (!valid_ctx(ctx) || !match_out || ctx->c.phase < 1) return SMP_ERR_INVALID_ARG;
+  Ctx &c = ctx->c;
+  DeviceGuard g(c.device);
+  if (c.phase < 3) {
+    // Precheck found the first choices distinct: the bulk and tail phases
+    // were skipped (AbsSmpEngine skips InitProc/CoreProc, smp_engine_abs.h:16-33).
+    if (!c.h_ctrl->perfect) return SMP_ERR_INVALID_ARG;
+    c.tail_ran = false;
+    int rc = c.d_match.ensure(sizeof(int32_t) * static_cast<size_t>(c.n));
+    if (!rc) rc = c.d_bid.ensure(sizeof(unsigned long long) * static_cast<size_t>(c.n));
+    if (rc) return rc;
+  }
+  if (cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  int rc = enqueue_post(c);
+  if (!rc) rc = copy_match_out(c, match_out, (flags & SMP_F_DEVICE_PTRS) != 0);
+  if (rc) return rc;
+  if (cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  rc = read_control(c);
+  if (!rc) rc = c.sync("post");
+  if (rc) return rc;
+  c.stats.post_ms = elapsed(c, kEvCoreEnd, kEvPostEnd);
+  fill_stats(c, false);
+  c.phase = 4;
+  c.stats.total_ms = c.stats.precheck_ms + c.stats.init_ms + c.stats.core_ms + c.stats.post_ms;
+  return control_status(c);
+}
+
+int smp_b200_stats(const smp_ctx *ctx, smp_stats *st) {
+  if (!valid_ctx(ctx) || !st) return SMP_ERR_INVALID_ARG;
+  *st = ctx->c.stats;
+  return SMP_OK;
+}
+
+int smp_b200_solve(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
+                   uint32_t flags, smp_stats *st) {
+  if (!valid_ctx(ctx) || !match_out) return SMP_ERR_INVALID_ARG;
+  Ctx &c = ctx->c;
+  DeviceGuard g(c.device);
+  int rc = do_stage(c, pref_m, pref_w, n, flags);
+  if (rc) return rc;
+  // One stream, no host round trips: kernels read ctrl->perfect themselves.
+  rc = enqueue_precheck(c, (flags & SMP_F_NO_PRECHECK) == 0);
+  if (!rc && (flags & SMP_F_VALIDATE)) rc = enqueue_validate(c);
+  if (!rc && cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = enqueue_init(c);
+  if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = enqueue_core(c);
+  if (!rc && cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = enqueue_post(c);
+  if (!rc && (flags & SMP_F_DEVICE_PTRS)) rc = copy_match_out(c, match_out, true);
+  if (!rc && cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc && !(flags & SMP_F_DEVICE_PTRS)) rc = copy_match_out(c, match_out, false);
+  if (!rc && (flags & SMP_F_CHECK)) {
+    if (cudaEventRecord(c.ev[kEvCheckBegin], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    // The checker reuses the solve's rank matrix; only a perfect instance
+    // (which skipped the inversion) builds it here.
+    if (!rc) rc = c.rank_bytes == 2 ? enqueue_invert<uint16_t>(c, c.pref_w, c.d_rank.as<uint16_t>(), kInvertIfPerfect)
+                                    : enqueue_invert<int32_t>(c, c.pref_w, c.d_rank.as<int32_t>(), kInvertIfPerfect);
+    if (!rc) rc = enqueue_check(c, c.d_match.as<int32_t>());
+    if (!rc && cudaEventRecord(c.ev[kEvCheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  }
+  if (!rc) rc = read_control(c);
+  if (!rc) rc = c.sync("solve");
+  if (rc) return rc;
+  c.phase = 3;
+  fill_stats(c, true);
+  c.phase = 4;
+  if (flags & SMP_F_CHECK) {
+    c.stats.blocking_pairs = static_cast<int64_t>(c.h_ctrl->blocking);
+    c.stats.check_ms = elapsed(c, kEvCheckBegin, kEvCheckEnd);
+    // The checker recounts the proposals from the matching itself.
+    if (c.h_ctrl->check_proposals != c.h_ctrl->proposals && c.h_ctrl->status == 0) {
+      c.last_error = "checker proposal count differs from the solve's";
+      return SMP_ERR_CUDA;
+    }
+  }
+  if (st) *st = c.stats;
+  return control_status(c);
+}
+
+int smp_b200_invert(smp_ctx *ctx, const int32_t *pref_w, int32_t n, int32_t *rank_out, uint32_t flags) {
+  if (!valid_ctx(ctx) || !pref_w || !rank_out || n <= 0 || n > SMP_B200_MAX_N) return SMP_ERR_INVALID_ARG;
+  Ctx &c = ctx->c;
+  DeviceGuard g(c.device);
+  c.n = n;
+  c.phase = 0;
+  c.staged = false;
+  c.rank_valid = false;
+  const size_t bytes = sizeof(int32_t) * static_cast<size_t>(n) * n;
+  int rc = c.d_ctrl.ensure(sizeof(Control));
+  if (rc) return rc;
+  const int32_t *src = pref_w;
+  int32_t *dst = rank_out;
+  if (!(flags & SMP_F_DEVICE_PTRS)) {
+    rc = c.d_pref_w.ensure(bytes);
+    if (!rc) rc = c.d_rank.ensure(bytes);
+    if (rc) return rc;
+    if (cudaMemcpyAsync(c.d_pref_w.ptr, pref_w, bytes, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+      return c.fail_cuda("pref_w copy");
+    src = c.d_pref_w.as<int32_t>();
+    dst = c.d_rank.as<int32_t>();
+  }
+  std::memset(c.h_ctrl, 0, sizeof(Control));
+  if (cudaMemcpyAsync(c.d_ctrl.ptr, c.h_ctrl, sizeof(Control), cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+    return c.fail_cuda("control reset");
+  if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  rc = enqueue_invert<int32_t>(c, src, dst, kInvertAlways);
+  if (rc) return rc;
+  if (cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  if (!(flags & SMP_F_DEVICE_PTRS)) {
+    if (cudaMemcpyAsync(rank_out, dst, bytes, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess)
+      return c.fail_cuda("rank copy");
+  }
+  rc = read_control(c);
+  if (!rc) rc = c.sync("invert");
+  if (rc) return rc;
+  c.stats = smp_stats{};
+  c.stats.n = n;
+  c.stats.blocking_pairs = -1;
+  c.stats.rank_bytes = 4;
+  c.stats.init_ms = elapsed(c, kEvPrecheckEnd, kEvInitEnd);
+  return control_status(c);
+}
+
+int smp_b200_check(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w, int32_t n, const int32_t *match,
+                   uint32_t flags, int64_t *blocking_pairs, int64_t *proposals) {
+  if (!valid_ctx(ctx) || !match) return SMP_ERR_INVALID_ARG;
+  Ctx &c = ctx->c;
+  DeviceGuard g(c.device);
+  int rc = do_stage(c, pref_m, pref_w, n, flags);
+  if (rc) return rc;
+  const int32_t *dmatch = match;
+  if (!(flags & SMP_F_DEVICE_PTRS)) {
+    rc = c.d_match.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+    if (rc) return rc;
+    if (cudaMemcpyAsync(c.d_match.ptr, match, sizeof(int32_t) * static_cast<size_t>(n), cudaMemcpyHostToDevice,
+                        c.stream) != cudaSuccess)
+      return c.fail_cuda("match copy");
+    dmatch = c.d_match.as<int32_t>();
+  }
+  rc = enqueue_precheck(c, false);
+  if (rc) return rc;
+  c.rank_bytes = rank_bytes_for(n);
+  rc = c.d_rank.ensure(static_cast<size_t>(n) * n * c.rank_bytes);
+  if (rc) return rc;
+  if (cudaEventRecord(c.ev[kEvCheckBegin], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  rc = c.rank_bytes == 2 ? enqueue_invert<uint16_t>(c, c.pref_w, c.d_rank.as<uint16_t>(), kInvertAlways)
+                         : enqueue_invert<int32_t>(c, c.pref_w, c.d_rank.as<int32_t>(), kInvertAlways);
+  if (!rc) rc = enqueue_check(c, dmatch);
+  if (rc) return rc;
+  if (cudaEventRecord(c.ev[kEvCheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  rc = read_control(c);
+  if (!rc) rc = c.sync("check");
+  if (rc) return rc;
+  c.stats.check_ms = elapsed(c, kEvCheckBegin, kEvCheckEnd);
+  const int s = control_status(c);
+  if (blocking_pairs) *blocking_pairs = s == 0 ? static_cast<int64_t>(c.h_ctrl->blocking) : -1;
+  if (proposals) *proposals = static_cast<int64_t>(c.h_ctrl->check_proposals);
+  c.phase = 0;
+  return s;
+}
+
+int smp_b200_generate(smp_ctx *ctx, int32_t kind, int32_t n, uint64_t seed, uint32_t salt, int32_t param,
+                      int32_t *pref_m, int32_t *pref_w, uint32_t flags) {
+  if (!valid_ctx(ctx) || !pref_m || !pref_w || n <= 0 || n > SMP_B200_MAX_N) return SMP_ERR_INVALID_ARG;
+  if (kind < SMP_GEN_UNIFORM || kind > SMP_GEN_SOLO) return SMP_ERR_INVALID_ARG;
+  if (kind == SMP_GEN_CORRELATED && (param < 0 || param > 10000)) return SMP_ERR_INVALID_ARG;
+  if (kind == SMP_GEN_GROUPED && param <= 0) return SMP_ERR_INVALID_ARG;
+  if (kind == SMP_GEN_SOLO && n < 3) return SMP_ERR_INVALID_ARG;
+  Ctx &c = ctx->c;
+  DeviceGuard g(c.device);
+  const size_t bytes = sizeof(int32_t) * static_cast<size_t>(n) * n;
+  int32_t *dm = pref_m, *dw = pref_w;
+  if (!(flags & SMP_F_DEVICE_PTRS)) {
+    int rc = c.d_pref_m.ensure(bytes);
+    if (!rc) rc = c.d_pref_w.ensure(bytes);
+    if (rc) return rc;
+    dm = c.d_pref_m.as<int32_t>();
+    dw = c.d_pref_w.as<int32_t>();
+  }
+  int rc = generate_side(c, kind, 0, n, seed, salt, param, dm);
+  if (!rc) rc = generate_side(c, kind, 1, n, seed, salt, param, dw);
+  if (rc) return rc;
+  if (!(flags & SMP_F_DEVICE_PTRS)) {
+    if (cudaMemcpyAsync(pref_m, dm, bytes, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess)
+      return c.fail_cuda("pref_m copy");
+    if (cudaMemcpyAsync(pref_w, dw, bytes, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess)
+      return c.fail_cuda("pref_w copy");
+  }
+  c.staged = false;
+  c.phase = 0;
+  return c.sync("generate");
+}
+
+}  // extern "C"

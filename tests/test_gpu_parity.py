@@ -1,0 +1,219 @@
+"""Parity of the CUDA path with the reference, through the C ABI.
+
+Integer work, so the bar is bit-exact: the matching must equal the one the
+reference's own engines returned (tests/golden), the proposal count must
+equal the reference's, and the GPU stability checker must find no blocking
+pair.  Full-size cases (n = 30000) are generated on the device by the
+library's generator; the SHA-256 of the generated lists must equal the
+digest recorded with the fixture, so the device inputs are the very inputs
+the reference solved.
+"""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+import oracle
+import pactae_b200 as pb
+from conftest import golden_match, load_cases
+
+pytestmark = pytest.mark.gpu
+
+CASES = load_cases()
+SMALL = [c for c in CASES if c["n"] <= 2000]
+FULL = [c for c in CASES if c["n"] > 2000]
+
+
+def sha(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.int32).tobytes()).hexdigest()
+
+
+def to_host(t) -> np.ndarray:
+    return t.cpu().numpy()
+
+
+# -- generator --------------------------------------------------------------
+GEN_CASES = [
+    (pb.SMP_GEN_UNIFORM, n, 0) for n in (1, 2, 7, 64, 1000)
+] + [
+    (pb.SMP_GEN_CONGESTED, 300, 0), (pb.SMP_GEN_CORRELATED, 301, 500), (pb.SMP_GEN_CORRELATED, 100, 0),
+    (pb.SMP_GEN_PERFECT, 200, 0), (pb.SMP_GEN_REF_CONGESTED, 150, 0), (pb.SMP_GEN_GROUPED, 250, 5),
+    (pb.SMP_GEN_GROUPED, 256, 64), (pb.SMP_GEN_SOLO, 3, 0), (pb.SMP_GEN_SOLO, 129, 0),
+]
+
+
+@pytest.mark.parametrize("kind,n,param", GEN_CASES)
+@pytest.mark.parametrize("salt", [0, 5])
+def test_device_generator_matches_oracle(ctx, kind, n, param, salt):
+    pm_d, pw_d = ctx.generate(kind, n, seed=77, salt=salt, param=param)
+    pm, pw = oracle.generate(kind, n, 77, salt, param)
+    assert np.array_equal(to_host(pm_d), pm)
+    assert np.array_equal(to_host(pw_d), pw)
+
+
+def test_generator_host_output(ctx):
+    pm, pw = ctx.generate(pb.SMP_GEN_UNIFORM, 300, seed=9, device=False)
+    opm, opw = oracle.generate(pb.SMP_GEN_UNIFORM, 300, 9)
+    assert np.array_equal(pm, opm) and np.array_equal(pw, opw)
+
+
+# -- solve vs the reference's matchings ------------------------------------
+@pytest.mark.parametrize("case", SMALL, ids=[c["name"] for c in SMALL])
+def test_solve_host_inputs_match_reference(ctx, case):
+    pm, pw = oracle.generate(case["kind"], case["n"], case["seed"], case["salt"], case["param"])
+    match, st = ctx.solve(pm, pw, check=True)
+    assert np.array_equal(match, golden_match(case["name"]))
+    assert st["proposals"] == case["proposals"]
+    assert st["blocking_pairs"] == 0
+
+
+@pytest.mark.parametrize("case", SMALL, ids=[c["name"] for c in SMALL])
+def test_solve_device_inputs_match_reference(ctx, case):
+    pm, pw = ctx.generate(case["kind"], case["n"], case["seed"], case["salt"], case["param"])
+    match, st = ctx.solve(pm, pw)
+    assert np.array_equal(to_host(match), golden_match(case["name"]))
+    assert st["proposals"] == case["proposals"]
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("case", FULL, ids=[c["name"] for c in FULL])
+def test_full_size_matches_reference(ctx, case):
+    import torch
+
+    pm, pw = ctx.generate(case["kind"], case["n"], case["seed"], case["salt"], case["param"])
+    assert sha(to_host(pm)) == case["sha256_pref_m"]
+    assert sha(to_host(pw)) == case["sha256_pref_w"]
+    match, st = ctx.solve(pm, pw, check=True)
+    assert sha(to_host(match)) == case["sha256_match"]
+    assert np.array_equal(to_host(match), golden_match(case["name"]))
+    assert st["proposals"] == case["proposals"]
+    assert st["blocking_pairs"] == 0
+    del pm, pw
+    torch.cuda.empty_cache()
+
+
+# -- configurations of the pipeline give the same answer ----------------------
+@pytest.mark.parametrize("prefix_k,tail", [(-1, -1), (-1, 0), (0, -1), (1, 0), (33, 1), (0, 200)])
+def test_pipeline_variants_agree(prefix_k, tail):
+    with pb.Context(prefix_k=prefix_k, tail_threshold=tail) as c:
+        for case in [x for x in SMALL if x["name"] in (
+                "uniform_n2000", "congested_n500", "correlated_n500", "uniform_n33", "solo_n100", "uniform_n1")]:
+            pm, pw = oracle.generate(case["kind"], case["n"], case["seed"], case["salt"], case["param"])
+            match, st = c.solve(pm, pw)
+            assert np.array_equal(match, golden_match(case["name"])), case["name"]
+            assert st["proposals"] == case["proposals"]
+
+
+def test_phase_api_and_engine_mirror(ctx):
+    case = next(c for c in SMALL if c["name"] == "uniform_n2000")
+    pm, pw = oracle.generate(case["kind"], case["n"], case["seed"], case["salt"], case["param"])
+    smp = pb.SmpObj.CreateFromFlatLists(pm.reshape(-1), pw.reshape(-1), case["n"])
+    eng = pb.SmpEngineB200(smp, case["n"], ctx=ctx)
+    match = eng.FindStableMatching()
+    assert match == golden_match(case["name"]).tolist()
+    st = ctx.stats()
+    assert st["proposals"] == case["proposals"] and st["perfect"] == 0
+    assert eng.init_time_ > 0 and eng.core_time_ > 0
+
+
+def test_perfect_instance_short_circuits(ctx):
+    case = next(c for c in SMALL if c["name"] == "perfect_n1000")
+    pm, pw = oracle.generate(case["kind"], case["n"], case["seed"], case["salt"], case["param"])
+    match, st = ctx.solve(pm, pw, check=True)
+    assert st["perfect"] == 1 and st["proposals"] == case["n"] and st["blocking_pairs"] == 0
+    assert np.array_equal(match, pm[:, 0])
+    # the phase API skips init and core, like AbsSmpEngine
+    smp = pb.SmpObj.CreateFromFlatLists(pm, pw, case["n"])
+    eng = pb.SmpEngineB200(smp, case["n"], ctx=ctx)
+    assert eng.FindStableMatching() == pm[:, 0].tolist()
+    assert eng.init_time_ == 0.0
+    # with the precheck off the full pipeline runs and agrees
+    match2, st2 = ctx.solve(pm, pw, precheck=False)
+    assert np.array_equal(match2, match) and st2["perfect"] == 0
+
+
+# -- inversion and checker ------------------------------------------------------
+@pytest.mark.parametrize("n", [1, 3, 5, 127, 1000])
+def test_invert_matches_oracle(ctx, n):
+    _, pw = oracle.generate(pb.SMP_GEN_UNIFORM, n, 31)
+    assert np.array_equal(ctx.invert(pw), oracle.invert(pw))
+
+
+def test_checker_counts_blocking_pairs(ctx):
+    pm, pw = oracle.generate(pb.SMP_GEN_UNIFORM, 500, 8)
+    m, props = oracle.gs_seq(pm, pw)
+    assert ctx.check(pm, pw, m) == (0, props)
+    for seed in range(3):
+        rng = np.random.default_rng(seed)
+        bad = m.copy()
+        i, j = rng.choice(500, 2, replace=False)
+        bad[[i, j]] = bad[[j, i]]
+        assert ctx.check(pm, pw, bad) == oracle.check(pm, pw, bad)
+    with pytest.raises(pb.SmpError) as e:
+        ctx.check(pm, pw, np.zeros(500, np.int32))
+    assert e.value.status == pb.SMP_ERR_INVALID_INPUT
+
+
+# -- invalid inputs are rejected, never run off the end ------------------------
+def test_invalid_inputs_rejected(ctx):
+    pm, pw = oracle.generate(pb.SMP_GEN_UNIFORM, 200, 3)
+    cases = []
+    bad = pw.copy()
+    bad[7, 3] = bad[7, 4]
+    cases.append((pm, bad, 0))                      # duplicate in a woman's row
+    bad = pw.copy()
+    bad[9, 0] = 5000
+    cases.append((pm, bad, 0))                      # out of range in a woman's row
+    bad = pm.copy()
+    bad[4, 0] = -1
+    cases.append((bad, pw, 0))                      # out of range first choice
+    bad = pm.copy()
+    bad[4, 5] = 200
+    cases.append((bad, pw, 0))                      # out of range inside the prefix
+    bad = pm.copy()
+    bad[4, 150] = bad[4, 151]
+    cases.append((bad, pw, pb.SMP_F_VALIDATE))      # duplicate caught by full validation
+    import ctypes
+    from pactae_b200 import _lib
+
+    for a, b, flags in cases:
+        a = np.ascontiguousarray(a, np.int32)
+        b = np.ascontiguousarray(b, np.int32)
+        out = np.empty(200, np.int32)
+        rc = _lib.lib.smp_b200_solve(ctx.handle, ctypes.c_void_p(a.ctypes.data), ctypes.c_void_p(b.ctypes.data),
+                                     200, ctypes.c_void_p(out.ctypes.data), flags, None)
+        assert rc == pb.SMP_ERR_INVALID_INPUT
+    # the context is still usable afterwards
+    match, _ = ctx.solve(pm, pw)
+    assert np.array_equal(match, oracle.gs_seq(pm, pw)[0])
+
+
+def test_bad_arguments(ctx):
+    with pytest.raises(pb.SmpError) as e:
+        ctx.generate(pb.SMP_GEN_SOLO, 2, seed=1)
+    assert e.value.status == pb.SMP_ERR_INVALID_ARG
+    import ctypes
+    from pactae_b200 import _lib
+
+    assert _lib.lib.smp_b200_solve(ctx.handle, None, None, 10, None, 0, None) == pb.SMP_ERR_INVALID_ARG
+    x = np.zeros(4, np.int32)
+    p = ctypes.c_void_p(x.ctypes.data)
+    assert _lib.lib.smp_b200_solve(ctx.handle, p, p, 0, p, 0, None) == pb.SMP_ERR_INVALID_ARG
+    assert _lib.lib.smp_b200_solve(ctx.handle, p, p, pb.SMP_B200_MAX_N + 1, p, 0, None) == pb.SMP_ERR_INVALID_ARG
+    assert _lib.lib.smp_b200_init(ctx.handle) in (pb.SMP_OK, pb.SMP_ERR_INVALID_ARG)
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_random_instances_against_oracle(ctx, seed):
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(2, 3000))
+    kind = int(rng.choice([pb.SMP_GEN_UNIFORM, pb.SMP_GEN_CONGESTED, pb.SMP_GEN_CORRELATED, pb.SMP_GEN_GROUPED]))
+    param = {pb.SMP_GEN_CORRELATED: int(rng.integers(0, 2000)), pb.SMP_GEN_GROUPED: int(rng.integers(1, 64))}.get(
+        kind, 0)
+    pm, pw = ctx.generate(kind, n, seed=seed + 500, param=param)
+    match, st = ctx.solve(pm, pw)
+    want, props = oracle.gs_seq(to_host(pm), to_host(pw))
+    assert np.array_equal(to_host(match), want)
+    assert st["proposals"] == props
