@@ -326,6 +326,10 @@ def run_b200(args, dist: Dist) -> dict | None:
             "solves_per_s": round(args.steps * dist.world / (total_ms * 1e-3), 2),
             "proposals": P,
             "tail_men": st0["tail_men"],
+            "tail_proposals": st0["tail_proposals"],
+            "bulk_hops": st0["bulk_hops"],
+            "tail_hops": st0["tail_hops"],
+            "tail_us_per_hop": round(st0["tail_ms"] * 1e3 / st0["tail_hops"], 4) if st0["tail_hops"] else None,
             "phase_ms": {k: round(st0[k], 4) for k in ("precheck_ms", "init_ms", "core_ms", "post_ms",
                                                          "invert_ms", "bulk_ms", "tail_ms")},
             "wall_s_timed_loop": round(t_wall, 3),

@@ -119,6 +119,8 @@ typedef struct smp_stats {
   int32_t tail_men;        /* free men handed to the tail kernel                   */
   int32_t rank_bytes;      /* bytes per rank-matrix entry (2 or 4)                  */
   int32_t kernel_launches; /* kernels the call launched                            */
+  int32_t bulk_hops;       /* accepted proposals in the all-SM kernel              */
+  int32_t tail_hops;       /* accepted proposals in the tail kernel                */
   int32_t reserved_i;
   float stage_ms;          /* host->device copy of the inputs                       */
   float precheck_ms;       /* device time of each phase (CUDA events)              */

@@ -77,6 +77,8 @@ class smp_stats(ctypes.Structure):
         ("tail_men", ctypes.c_int32),
         ("rank_bytes", ctypes.c_int32),
         ("kernel_launches", ctypes.c_int32),
+        ("bulk_hops", ctypes.c_int32),
+        ("tail_hops", ctypes.c_int32),
         ("reserved_i", ctypes.c_int32),
         ("stage_ms", ctypes.c_float),
         ("precheck_ms", ctypes.c_float),

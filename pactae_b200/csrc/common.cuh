@@ -30,7 +30,8 @@ struct Control {
   unsigned long long check_proposals;  // checker: proposals recounted from the matching
   unsigned long long bulk_proposals;   // proposals settled by k_bulk
   unsigned long long tail_proposals;   // proposals settled by k_tail
-  unsigned long long pad1;
+  unsigned int bulk_hops;              // accepted proposals in k_bulk
+  unsigned int tail_hops;              // accepted proposals in k_tail
 };
 
 __device__ __forceinline__ void report(Control *ctrl, int status, int value) {

@@ -304,6 +304,8 @@ int do_stage(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, ui
 void fill_stats(Ctx &c, bool timed_phases) {
   c.stats.proposals = static_cast<int64_t>(c.h_ctrl->proposals);
   c.stats.tail_proposals = static_cast<int64_t>(c.h_ctrl->tail_proposals);
+  c.stats.bulk_hops = static_cast<int32_t>(c.h_ctrl->bulk_hops);
+  c.stats.tail_hops = static_cast<int32_t>(c.h_ctrl->tail_hops);
   c.stats.perfect = c.h_ctrl->perfect;
   c.stats.tail_men = c.tail_ran ? c.h_ctrl->tail_men : 0;
   c.stats.rank_bytes = c.rank_bytes;

@@ -295,6 +295,7 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
   const int lane = threadIdx.x & 31;
   int m = -1, pos = 0;
   unsigned long long settled = 0;  // proposals this warp decided (lane 0's copy is used)
+  unsigned int hops = 0;           // proposals this warp saw accepted
   for (;;) {
     int free_now = 0;
     if (m < 0) {
@@ -344,6 +345,7 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
       const uint32_t rkj = __shfl_sync(kFullMask, rk, j);
       if (bid_rank(old) > rkj) {  // accepted: she was free or held a worse man
         settled += j + 1;
+        hops++;
         if (old == kFree) {
           if (lane == 0) atomicSub(&ctrl->free_count, 1);
           m = -1;
@@ -365,7 +367,10 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
       }
     }
   }
-  if (lane == 0 && settled) atomicAdd(&ctrl->bulk_proposals, settled);
+  if (lane == 0 && settled) {
+    atomicAdd(&ctrl->bulk_proposals, settled);
+    atomicAdd(&ctrl->bulk_hops, hops);
+  }
 }
 
 // Largest n whose tail state (4-byte bid + 2-byte position per person) fits
@@ -434,6 +439,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
 
   int m = -1, pos = 0;
   unsigned long long settled = 0;
+  unsigned int hops = 0;
   for (;;) {
     if (m < 0) {
       int i = 0;
@@ -477,6 +483,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
       const uint32_t rkj = __shfl_sync(kFullMask, rk, j);
       if ((old >> 16) > rkj) {
         settled += j + 1;
+        hops++;
         if (old == 0xFFFFFFFFu) {
           m = -1;
         } else {
@@ -497,7 +504,10 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
       }
     }
   }
-  if (lane == 0 && settled) atomicAdd(&ctrl->tail_proposals, settled);
+  if (lane == 0 && settled) {
+    atomicAdd(&ctrl->tail_proposals, settled);
+    atomicAdd(&ctrl->tail_hops, hops);
+  }
   __syncthreads();
 
   unsigned long long props = 0;
