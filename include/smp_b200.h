@@ -104,10 +104,13 @@ typedef struct smp_cfg {
                            /* -1 = none                                             */
   int32_t tail_threshold;  /* free men at which the single-CTA tail takes over;     */
                            /* 0 = auto, -1 = never                                  */
-  int32_t reserved0;
+  int32_t bulk_window;     /* widest look-ahead of the all-SM kernel, in choices    */
+                           /* per warp step (32, 64, 128, 256); 0 = auto            */
   uint64_t hbm_budget;     /* bytes the batch / serving paths may hold resident;    */
                            /* 0 = 64 GiB                                            */
-  uint64_t reserved1[4];
+  int32_t tail_window;     /* the same for the tail kernel; 0 = auto                */
+  int32_t mode;            /* 0 = auto, 1 = rank-matrix mode only                   */
+  uint64_t reserved[3];
 } smp_cfg;
 
 typedef struct smp_stats {
@@ -121,7 +124,7 @@ typedef struct smp_stats {
   int32_t kernel_launches; /* kernels the call launched                            */
   int32_t bulk_hops;       /* accepted proposals in the all-SM kernel              */
   int32_t tail_hops;       /* accepted proposals in the tail kernel                */
-  int32_t reserved_i;
+  int32_t mode;            /* 0 rank-matrix mode, 1 query mode, 2 query then rank  */
   float stage_ms;          /* host->device copy of the inputs                       */
   float precheck_ms;       /* device time of each phase (CUDA events)              */
   float init_ms;
@@ -129,7 +132,7 @@ typedef struct smp_stats {
   float post_ms;
   float check_ms;
   float total_ms;          /* precheck + init + core + post                        */
-  float invert_ms;         /* rank inversion kernel (part of init)                 */
+  float invert_ms;         /* rank inversion / prefix query kernels (part of init) */
   float bulk_ms;           /* all-SM proposal kernel (part of core)                */
   float tail_ms;           /* single-CTA tail kernel (part of core)                */
   float reserved[2];

@@ -87,12 +87,16 @@ class Context:
     """One solver context (smp_ctx): a CUDA stream plus grow-only device
     buffers on one device.  Not thread-safe; use one per thread."""
 
-    def __init__(self, device: int = 0, prefix_k: int = 0, tail_threshold: int = 0, hbm_budget: int = 0):
+    def __init__(self, device: int = 0, prefix_k: int = 0, tail_threshold: int = 0, hbm_budget: int = 0,
+                 bulk_window: int = 0, tail_window: int = 0, mode: int = 0):
         cfg = smp_cfg()
         cfg.device = device
         cfg.prefix_k = prefix_k
         cfg.tail_threshold = tail_threshold
         cfg.hbm_budget = hbm_budget
+        cfg.bulk_window = bulk_window
+        cfg.tail_window = tail_window
+        cfg.mode = mode
         handle = ctypes.c_void_p()
         _check(lib.smp_b200_create(ctypes.byref(handle), ctypes.byref(cfg)), "smp_b200_create")
         self._h = handle

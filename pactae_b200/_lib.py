@@ -61,9 +61,11 @@ class smp_cfg(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("prefix_k", ctypes.c_int32),
         ("tail_threshold", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("bulk_window", ctypes.c_int32),
         ("hbm_budget", ctypes.c_uint64),
-        ("reserved1", ctypes.c_uint64 * 4),
+        ("tail_window", ctypes.c_int32),
+        ("mode", ctypes.c_int32),
+        ("reserved", ctypes.c_uint64 * 3),
     ]
 
 
@@ -79,7 +81,7 @@ class smp_stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_int32),
         ("bulk_hops", ctypes.c_int32),
         ("tail_hops", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32),
+        ("mode", ctypes.c_int32),
         ("stage_ms", ctypes.c_float),
         ("precheck_ms", ctypes.c_float),
         ("init_ms", ctypes.c_float),

@@ -14,19 +14,30 @@ constexpr unsigned kFullMask = 0xFFFFFFFFu;
 constexpr int kStatusOk = 0;
 constexpr int kStatusInvalidInput = 2;
 
+// Modes of one solve, chosen on the device by the precheck.
+constexpr int kModeRank = 0;   // rank matrix, prefix gathered from it; any instance
+constexpr int kModeQuery = 1;  // prefix answered straight from pref_w rows, no rank matrix
+
 // Per-solve control block in device memory.  Kernels of one solve share it;
-// the host zeroes it (and sets free_count = n, perfect = 1) before the solve.
+// the host writes its initial value (free_count = n, the allow_* switches)
+// before the solve.
 struct Control {
-  int32_t status;        // first error a kernel saw (kStatus*), 0 if none
-  int32_t perfect;       // 1 while every first choice seen so far is distinct
-  int32_t next_man;      // bulk kernel: next man that has not proposed yet
-  int32_t free_count;    // women that have not received a proposal yet
-  int32_t tail_count;    // men handed from the bulk kernel to the tail kernel
-  int32_t tail_men;      // men the tail kernel started chains for
-  int32_t bad_value;     // first out-of-range preference value seen
-  int32_t pad0;
-  unsigned long long proposals;  // sum over men of (final position + 1)
-  unsigned long long blocking;   // checker: blocking pairs
+  int32_t status;         // first error a kernel saw (kStatus*), 0 if none
+  int32_t perfect;        // precheck: every first choice distinct (and allowed)
+  int32_t next_man;       // bulk kernel: next man that has not proposed yet
+  int32_t free_count;     // women that have not received a proposal yet
+  int32_t tail_count;     // men handed from the bulk kernel to the tail kernel
+  int32_t tail_men;       // men the tail kernel started chains for
+  int32_t bad_value;      // first out-of-range preference value seen
+  int32_t mode;           // kModeRank or kModeQuery
+  int32_t retry;          // query mode met a man beyond his prefix: rerun in rank mode
+  int32_t allow_perfect;  // host switch: 0 disables the distinct-first-choices shortcut
+  int32_t allow_query;    // host switch: 1 if the query mode may be chosen
+  int32_t blocks_done;    // precheck: blocks that finished (the last one decides)
+  int32_t distinct;       // precheck: number of distinct first choices
+  int32_t pad0[3];
+  unsigned long long proposals;        // sum over men of (final position + 1)
+  unsigned long long blocking;         // checker: blocking pairs
   unsigned long long check_proposals;  // checker: proposals recounted from the matching
   unsigned long long bulk_proposals;   // proposals settled by k_bulk
   unsigned long long tail_proposals;   // proposals settled by k_tail

@@ -61,6 +61,9 @@ struct Ctx {
   size_t smem_optin = 0;  // max dynamic shared memory per block
   int prefix_k_cfg = 0;
   int tail_threshold_cfg = 0;
+  int bulk_window_cfg = 0;
+  int tail_window_cfg = 0;
+  int mode_cfg = 0;
   uint64_t hbm_budget = 64ull << 30;
   std::string last_error;
 
@@ -71,6 +74,9 @@ struct Ctx {
   const int32_t *pref_w = nullptr;
   int K = 0;               // prefix width (0 = none)
   int tail_threshold = 0;  // 0 = tail kernel disabled
+  bool query_ok = false;   // the query mode may be chosen for this n
+  int bulk_window = 256;   // look-ahead choices per warp step
+  int tail_window = 256;
   int rank_bytes = 2;
   bool rank_valid = false;  // d_rank holds the inversion of pref_w
   bool tail_ran = false;
@@ -78,6 +84,7 @@ struct Ctx {
 
   DeviceBuf d_pref_m, d_pref_w, d_rank, d_prefix, d_bid, d_tailq, d_seen, d_ctrl, d_match;
   DeviceBuf d_husband, d_prank;
+  DeviceBuf d_qcnt, d_qoff, d_qlist;
   DeviceBuf gen_keys_a, gen_keys_b, gen_seg, gen_temp, gen_aux;
   Control *h_ctrl = nullptr;  // pinned host copy of the control block
   cudaEvent_t ev[10] = {};

@@ -13,8 +13,10 @@ using namespace smpb200;
 
 namespace {
 
-constexpr int kDefaultPrefixK = 128;
-constexpr int kDefaultTailThreshold = 32;
+constexpr int kDefaultPrefixK = 192;
+constexpr int kDefaultTailThreshold = 96;
+constexpr int kDefaultBulkWindow = 256;
+constexpr int kDefaultTailWindow = 256;
 constexpr int kU16MaxN = 65535;
 
 inline bool valid_ctx(const smp_ctx *ctx) { return ctx != nullptr && ctx->c.stream != nullptr; }
@@ -44,19 +46,25 @@ float elapsed(const Ctx &c, int a, int b) {
 
 int rank_bytes_for(int n) { return n <= kU16MaxN ? 2 : 4; }
 
-// Blocks per SM that k_bulk can keep resident.
-template <typename RankT>
-int bulk_grid(const Ctx &c) {
+// Blocks per SM that a kernel can keep resident at the given block size.
+template <typename Kernel>
+int resident_grid(const Ctx &c, Kernel kernel, int block) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bulk<RankT>, 256, 0) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess) {
     cudaGetLastError();
     per_sm = 4;
   }
   return c.sm_count * std::max(per_sm, 1);
 }
 
-// --------------------------------------------------------------------------
-// Phase bodies (enqueue only; the public entry points add sync + readback).
+// Number of 32-choice windows for a configured look-ahead (choices).
+int subs_for(int window) {
+  if (window <= 32) return 1;
+  if (window <= 64) return 2;
+  if (window <= 128) return 4;
+  return 8;
+}
+
 // --------------------------------------------------------------------------
 // SMP_F_VALIDATE: both lists, every row a permutation.
 int enqueue_validate(Ctx &c) {
@@ -76,97 +84,187 @@ int enqueue_validate(Ctx &c) {
   return c.check_launch("k_validate_rows");
 }
 
-int enqueue_precheck(Ctx &c, bool run_precheck) {
+// Per-solve plan, fixed once n is known: rank width, prefix width, whether
+// the query mode may run, and the tail threshold.
+void plan(Ctx &c) {
   const int n = c.n;
-  Control init = {};
-  init.perfect = run_precheck ? 1 : 0;
-  init.free_count = n;
-  std::memcpy(c.h_ctrl, &init, sizeof(Control));
-  if (cudaMemcpyAsync(c.d_ctrl.ptr, c.h_ctrl, sizeof(Control), cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
-    return c.fail_cuda("control reset");
-  if (run_precheck) {
-    const size_t words = (static_cast<size_t>(n) + 31) / 32;
-    if (cudaMemsetAsync(c.d_seen.ptr, 0, words * 4, c.stream) != cudaSuccess) return c.fail_cuda("seen reset");
-    const int grid = std::min(c.sm_count * 4, (n + 255) / 256);
-    k_precheck<<<grid, 256, 0, c.stream>>>(c.pref_m, n, c.d_seen.as<uint32_t>(), c.d_ctrl.as<Control>());
-    c.launches++;
-    return c.check_launch("k_precheck");
-  }
-  return SMP_OK;
-}
-
-template <typename RankT>
-int enqueue_invert(Ctx &c, const int32_t *pref_w, RankT *rank, int mode) {
-  const int n = c.n;
-  const size_t smem = static_cast<size_t>(n) * sizeof(RankT);
-  const size_t smem_padded = (smem + 15) & ~static_cast<size_t>(15);
-  if (smem_padded <= c.smem_optin) {
-    if (cudaFuncSetAttribute(k_invert<RankT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem_padded)) != cudaSuccess)
-      return c.fail_cuda("k_invert smem attribute");
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_invert<RankT>, 512, smem_padded) != cudaSuccess) {
-      cudaGetLastError();
-      per_sm = 1;
-    }
-    const int grid = std::min(n, c.sm_count * std::max(per_sm, 1));
-    k_invert<RankT><<<grid, 512, smem_padded, c.stream>>>(pref_w, rank, n, c.d_ctrl.as<Control>(), mode);
-    c.launches++;
-    return c.check_launch("k_invert");
-  }
-  // Rows too long for shared memory (int32 ranks only).
-  int32_t *r32 = reinterpret_cast<int32_t *>(rank);
-  k_invert_global<<<c.sm_count * 8, 256, 0, c.stream>>>(pref_w, r32, n, c.d_ctrl.as<Control>(), mode);
-  c.launches++;
-  int rc = c.check_launch("k_invert_global");
-  if (rc) return rc;
-  k_invert_verify<<<c.sm_count * 8, 256, 0, c.stream>>>(pref_w, r32, n, c.d_ctrl.as<Control>(), mode);
-  c.launches++;
-  return c.check_launch("k_invert_verify");
-}
-
-int enqueue_init(Ctx &c) {
-  const int n = c.n;
-  const size_t nn = static_cast<size_t>(n) * n;
   c.rank_bytes = rank_bytes_for(n);
-  int rc = c.d_rank.ensure(nn * c.rank_bytes);
-  if (!rc) rc = c.d_bid.ensure(sizeof(unsigned long long) * n);
-  if (rc) return rc;
-  // Prefix width and tail eligibility.
   c.K = 0;
   if (c.rank_bytes == 2 && c.prefix_k_cfg >= 0) {
     const int want = c.prefix_k_cfg > 0 ? c.prefix_k_cfg : kDefaultPrefixK;
     c.K = std::min(want, n);
   }
-  if (c.K > 0) {
-    rc = c.d_prefix.ensure(sizeof(uint32_t) * static_cast<size_t>(n) * c.K);
-    if (rc) return rc;
-  }
+  c.query_ok = c.mode_cfg != 1 && c.K > 0 && n <= kU16MaxN && row_smem_bytes<uint16_t>(n) <= c.smem_optin;
+  c.bulk_window = c.bulk_window_cfg > 0 ? c.bulk_window_cfg : kDefaultBulkWindow;
+  c.tail_window = c.tail_window_cfg > 0 ? c.tail_window_cfg : kDefaultTailWindow;
   c.tail_threshold = 0;
-  if (c.tail_threshold_cfg >= 0 && n <= kU16MaxN && tail_smem_bytes(n) <= c.smem_optin) {
+  if (c.tail_threshold_cfg >= 0 && n <= kU16MaxN && tail_smem_bytes(n) <= c.smem_optin)
     c.tail_threshold = c.tail_threshold_cfg > 0 ? c.tail_threshold_cfg : kDefaultTailThreshold;
+}
+
+int enqueue_precheck(Ctx &c, bool allow_perfect) {
+  const int n = c.n;
+  Control init = {};
+  init.free_count = n;
+  init.allow_perfect = allow_perfect ? 1 : 0;
+  init.allow_query = c.query_ok ? 1 : 0;
+  std::memcpy(c.h_ctrl, &init, sizeof(Control));
+  if (cudaMemcpyAsync(c.d_ctrl.ptr, c.h_ctrl, sizeof(Control), cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+    return c.fail_cuda("control reset");
+  const size_t words = (static_cast<size_t>(n) + 31) / 32;
+  if (cudaMemsetAsync(c.d_seen.ptr, 0, words * 4, c.stream) != cudaSuccess) return c.fail_cuda("seen reset");
+  const int grid = std::max(1, std::min(c.sm_count * 4, (n + 255) / 256));
+  k_precheck<<<grid, 256, 0, c.stream>>>(c.pref_m, n, c.d_seen.as<uint32_t>(), c.d_ctrl.as<Control>());
+  c.launches++;
+  return c.check_launch("k_precheck");
+}
+
+template <typename RankT>
+int enqueue_invert(Ctx &c, const int32_t *pref_w, RankT *rank, int gate) {
+  const int n = c.n;
+  const size_t smem = row_smem_bytes<RankT>(n);
+  if (smem <= c.smem_optin) {
+    if (cudaFuncSetAttribute(k_invert<RankT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess)
+      return c.fail_cuda("k_invert smem attribute");
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_invert<RankT>, 512, smem) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    const int grid = std::min(n, c.sm_count * std::max(per_sm, 1));
+    k_invert<RankT><<<grid, 512, smem, c.stream>>>(pref_w, rank, n, c.d_ctrl.as<Control>(), gate);
+    c.launches++;
+    return c.check_launch("k_invert");
   }
+  // Rows too long for shared memory (int32 ranks only).
+  int32_t *r32 = reinterpret_cast<int32_t *>(rank);
+  k_invert_global<<<c.sm_count * 8, 256, 0, c.stream>>>(pref_w, r32, n, c.d_ctrl.as<Control>(), gate);
+  c.launches++;
+  int rc = c.check_launch("k_invert_global");
+  if (rc) return rc;
+  k_invert_verify<<<c.sm_count * 8, 256, 0, c.stream>>>(pref_w, r32, n, c.d_ctrl.as<Control>(), gate);
+  c.launches++;
+  return c.check_launch("k_invert_verify");
+}
+
+int enqueue_invert_any(Ctx &c, int gate) {
+  return c.rank_bytes == 2 ? enqueue_invert<uint16_t>(c, c.pref_w, c.d_rank.as<uint16_t>(), gate)
+                           : enqueue_invert<int32_t>(c, c.pref_w, c.d_rank.as<int32_t>(), gate);
+}
+
+int enqueue_prefix_gather(Ctx &c, int gate) {
+  if (c.K <= 0) return SMP_OK;
+  const int n = c.n;
+  const size_t total = static_cast<size_t>(n) * c.K;
+  const int grid = static_cast<int>(std::min<size_t>(static_cast<size_t>(c.sm_count) * 16, (total + 255) / 256));
+  k_prefix<<<grid, 256, 0, c.stream>>>(c.pref_m, c.d_rank.as<uint16_t>(), c.d_prefix.as<uint32_t>(), n, c.K,
+                                       c.d_ctrl.as<Control>(), gate);
+  c.launches++;
+  return c.check_launch("k_prefix");
+}
+
+// Query mode: bucket the (man, position) pairs of every man's first K
+// choices by woman, then answer them from each woman's row.
+int enqueue_query(Ctx &c) {
+  const int n = c.n;
+  const size_t total = static_cast<size_t>(n) * c.K;
+  int rc = c.d_qcnt.ensure(sizeof(int32_t) * (static_cast<size_t>(n) + 1));
+  if (!rc) rc = c.d_qoff.ensure(sizeof(int32_t) * (static_cast<size_t>(n) + 1));
+  if (!rc) rc = c.d_qlist.ensure(sizeof(uint32_t) * total);
+  if (rc) return rc;
+  if (cudaMemsetAsync(c.d_qcnt.ptr, 0, sizeof(int32_t) * (static_cast<size_t>(n) + 1), c.stream) != cudaSuccess)
+    return c.fail_cuda("qcnt reset");
+  Control *ctrl = c.d_ctrl.as<Control>();
+  const int grid = static_cast<int>(std::min<size_t>(static_cast<size_t>(c.sm_count) * 16, (total + 255) / 256));
+  k_qcount<<<grid, 256, 0, c.stream>>>(c.pref_m, n, c.K, c.d_qcnt.as<int32_t>(), ctrl);
+  k_qscan<<<1, 1024, 0, c.stream>>>(c.d_qcnt.as<int32_t>(), c.d_qoff.as<int32_t>(), n, ctrl);
+  k_qscatter<<<grid, 256, 0, c.stream>>>(c.pref_m, n, c.K, c.d_qoff.as<int32_t>(), c.d_qcnt.as<int32_t>(),
+                                         c.d_qlist.as<uint32_t>(), ctrl);
+  c.launches += 3;
+  rc = c.check_launch("k_qcount/k_qscan/k_qscatter");
+  if (rc) return rc;
+  const size_t smem = row_smem_bytes<uint16_t>(n);
+  if (cudaFuncSetAttribute(k_qinvert, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+      cudaSuccess)
+    return c.fail_cuda("k_qinvert smem attribute");
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_qinvert, 512, smem) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const int qgrid = std::min(n, c.sm_count * std::max(per_sm, 1));
+  k_qinvert<<<qgrid, 512, smem, c.stream>>>(c.pref_w, n, c.K, c.d_qoff.as<int32_t>(), c.d_qlist.as<uint32_t>(),
+                                            c.d_prefix.as<uint32_t>(), ctrl);
+  c.launches++;
+  return c.check_launch("k_qinvert");
+}
+
+int enqueue_init(Ctx &c) {
+  const int n = c.n;
+  const size_t nn = static_cast<size_t>(n) * n;
+  int rc = c.d_rank.ensure(nn * c.rank_bytes);
+  if (!rc) rc = c.d_bid.ensure(sizeof(unsigned long long) * n);
+  if (!rc && c.K > 0) rc = c.d_prefix.ensure(sizeof(uint32_t) * static_cast<size_t>(n) * c.K);
+  if (rc) return rc;
   // Every woman starts free (SmpEngineBamboo::InitProc fills partner_rank
   // with n, smp_engine_bamboo.cu:37).
   if (cudaMemsetAsync(c.d_bid.ptr, 0xFF, sizeof(unsigned long long) * n, c.stream) != cudaSuccess)
     return c.fail_cuda("bid reset");
-  if (c.rank_bytes == 2) {
-    rc = enqueue_invert<uint16_t>(c, c.pref_w, c.d_rank.as<uint16_t>(), kInvertUnlessPerfect);
-  } else {
-    rc = enqueue_invert<int32_t>(c, c.pref_w, c.d_rank.as<int32_t>(), kInvertUnlessPerfect);
+  if (c.query_ok) {
+    rc = enqueue_query(c);
+    if (rc) return rc;
   }
+  rc = enqueue_invert_any(c, kGateModeRank);
   if (rc) return rc;
   if (cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
-  c.rank_valid = true;
-  if (c.K > 0) {
-    const size_t total = static_cast<size_t>(n) * c.K;
-    const int grid = static_cast<int>(std::min<size_t>(static_cast<size_t>(c.sm_count) * 16, (total + 255) / 256));
-    k_prefix<<<grid, 256, 0, c.stream>>>(c.pref_m, c.d_rank.as<uint16_t>(), c.d_prefix.as<uint32_t>(), n, c.K,
-                                         c.d_ctrl.as<Control>());
-    c.launches++;
-    rc = c.check_launch("k_prefix");
+  return enqueue_prefix_gather(c, kGateModeRank);
+}
+
+template <typename RankT, int kSub>
+int launch_bulk(Ctx &c, int round) {
+  const RankT *rank = reinterpret_cast<const RankT *>(c.d_rank.ptr);
+  const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
+  k_bulk<RankT, kSub><<<resident_grid(c, k_bulk<RankT, kSub>, 256), 256, 0, c.stream>>>(
+      c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(), c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
+      c.n, c.tail_threshold, round);
+  c.launches++;
+  return c.check_launch("k_bulk");
+}
+
+template <typename RankT, int kSub>
+int launch_tail(Ctx &c, int round) {
+  const RankT *rank = reinterpret_cast<const RankT *>(c.d_rank.ptr);
+  const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
+  const size_t smem = tail_smem_bytes(c.n);
+  if (cudaFuncSetAttribute(k_tail<RankT, kSub>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess)
+    return c.fail_cuda("k_tail smem attribute");
+  k_tail<RankT, kSub><<<1, 1024, smem, c.stream>>>(c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(),
+                                                   c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
+                                                   c.d_match.as<int32_t>(), c.n, round);
+  c.launches++;
+  return c.check_launch("k_tail");
+}
+
+template <typename RankT>
+int enqueue_round(Ctx &c, int round) {
+  int rc;
+  switch (subs_for(c.bulk_window)) {
+    case 1: rc = launch_bulk<RankT, 1>(c, round); break;
+    case 2: rc = launch_bulk<RankT, 2>(c, round); break;
+    case 4: rc = launch_bulk<RankT, 4>(c, round); break;
+    default: rc = launch_bulk<RankT, 8>(c, round); break;
   }
-  return rc;
+  if (rc) return rc;
+  if (round == 0 && cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  if (c.tail_threshold <= 0) return SMP_OK;
+  switch (subs_for(c.tail_window)) {
+    case 1: return launch_tail<RankT, 1>(c, round);
+    case 2: return launch_tail<RankT, 2>(c, round);
+    case 4: return launch_tail<RankT, 4>(c, round);
+    default: return launch_tail<RankT, 8>(c, round);
+  }
 }
 
 template <typename RankT>
@@ -175,28 +273,17 @@ int enqueue_core_t(Ctx &c) {
   int rc = c.d_tailq.ensure(sizeof(int2) * static_cast<size_t>(n));
   if (!rc) rc = c.d_match.ensure(sizeof(int32_t) * static_cast<size_t>(n));
   if (rc) return rc;
-  const RankT *rank = reinterpret_cast<const RankT *>(c.d_rank.ptr);
-  const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
-  k_bulk<RankT><<<bulk_grid<RankT>(c), 256, 0, c.stream>>>(c.pref_m, rank, prefix, c.K,
-                                                           c.d_bid.as<unsigned long long>(), c.d_ctrl.as<Control>(),
-                                                           c.d_tailq.as<int2>(), n, c.tail_threshold);
+  c.tail_ran = c.tail_threshold > 0;
+  rc = enqueue_round<RankT>(c, 0);
+  if (rc || !c.query_ok) return rc;
+  // Rank-mode retry round; every kernel of it returns at once unless the
+  // query mode stopped because a man went beyond his prefix.
+  k_retry_reset<<<1, 1024, 0, c.stream>>>(c.d_bid.as<unsigned long long>(), n, c.d_ctrl.as<Control>());
   c.launches++;
-  rc = c.check_launch("k_bulk");
-  if (rc) return rc;
-  if (cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
-  c.tail_ran = false;
-  if (c.tail_threshold > 0) {
-    const size_t smem = tail_smem_bytes(n);
-    if (cudaFuncSetAttribute(k_tail<RankT>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
-        cudaSuccess)
-      return c.fail_cuda("k_tail smem attribute");
-    k_tail<RankT><<<1, 1024, smem, c.stream>>>(c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(),
-                                               c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
-                                               c.d_match.as<int32_t>(), n);
-    c.launches++;
-    rc = c.check_launch("k_tail");
-    c.tail_ran = true;
-  }
+  rc = c.check_launch("k_retry_reset");
+  if (!rc) rc = enqueue_invert_any(c, kGateRetry);
+  if (!rc) rc = enqueue_prefix_gather(c, kGateRetry);
+  if (!rc) rc = enqueue_round<RankT>(c, 1);
   return rc;
 }
 
@@ -207,7 +294,7 @@ int enqueue_post(Ctx &c) {
   const int n = c.n;
   int rc = c.d_match.ensure(sizeof(int32_t) * static_cast<size_t>(n));
   if (rc) return rc;
-  const int grid = std::min(c.sm_count * 4, (n + 255) / 256);
+  const int grid = std::max(1, std::min(c.sm_count * 4, (n + 255) / 256));
   k_match<<<grid, 256, 0, c.stream>>>(c.pref_m, c.d_bid.as<unsigned long long>(), c.d_match.as<int32_t>(), n,
                                       c.d_ctrl.as<Control>());
   c.launches++;
@@ -248,11 +335,11 @@ int enqueue_check_t(Ctx &c, const int32_t *match) {
   if (rc) return rc;
   if (cudaMemsetAsync(c.d_husband.ptr, 0xFF, sizeof(int32_t) * static_cast<size_t>(n), c.stream) != cudaSuccess)
     return c.fail_cuda("husband reset");
-  const int grid = std::min(c.sm_count * 4, (n + 255) / 256);
+  const int grid = std::max(1, std::min(c.sm_count * 4, (n + 255) / 256));
   k_check_husband<<<grid, 256, 0, c.stream>>>(match, c.d_husband.as<int32_t>(), n, c.d_ctrl.as<Control>());
   k_check_prank<RankT><<<grid, 256, 0, c.stream>>>(c.d_husband.as<int32_t>(), reinterpret_cast<const RankT *>(c.d_rank.ptr),
                                                   c.d_prank.as<int32_t>(), n, c.d_ctrl.as<Control>());
-  const int sgrid = std::min(c.sm_count * 8, (n * 32 + 255) / 256);
+  const int sgrid = std::max(1, std::min(c.sm_count * 8, (n * 32 + 255) / 256));
   k_check_scan<RankT><<<sgrid, 256, 0, c.stream>>>(c.pref_m, reinterpret_cast<const RankT *>(c.d_rank.ptr), match,
                                                   c.d_prank.as<int32_t>(), n, c.d_ctrl.as<Control>());
   c.launches += 3;
@@ -277,6 +364,7 @@ int do_stage(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, ui
   c.stats.n = n;
   c.stats.blocking_pairs = -1;
   c.launches = 0;
+  plan(c);
   int rc = c.d_ctrl.ensure(sizeof(Control));
   if (!rc) rc = c.d_seen.ensure(((static_cast<size_t>(n) + 31) / 32) * 4);
   if (rc) return rc;
@@ -307,6 +395,7 @@ void fill_stats(Ctx &c, bool timed_phases) {
   c.stats.bulk_hops = static_cast<int32_t>(c.h_ctrl->bulk_hops);
   c.stats.tail_hops = static_cast<int32_t>(c.h_ctrl->tail_hops);
   c.stats.perfect = c.h_ctrl->perfect;
+  c.stats.mode = c.h_ctrl->retry ? 2 : c.h_ctrl->mode;
   c.stats.tail_men = c.tail_ran ? c.h_ctrl->tail_men : 0;
   c.stats.rank_bytes = c.rank_bytes;
   c.stats.kernel_launches = c.launches;
@@ -360,6 +449,9 @@ int smp_b200_create(smp_ctx **out, const smp_cfg *cfg) {
     c.device = cfg->device;
     c.prefix_k_cfg = cfg->prefix_k;
     c.tail_threshold_cfg = cfg->tail_threshold;
+    c.bulk_window_cfg = cfg->bulk_window;
+    c.tail_window_cfg = cfg->tail_window;
+    c.mode_cfg = cfg->mode;
     if (cfg->hbm_budget) c.hbm_budget = cfg->hbm_budget;
   }
   int count = 0;
@@ -403,8 +495,8 @@ void smp_b200_destroy(smp_ctx *ctx) {
     DeviceGuard g(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
     for (DeviceBuf *b : {&c.d_pref_m, &c.d_pref_w, &c.d_rank, &c.d_prefix, &c.d_bid, &c.d_tailq, &c.d_seen,
-                         &c.d_ctrl, &c.d_match, &c.d_husband, &c.d_prank, &c.gen_keys_a, &c.gen_keys_b, &c.gen_seg,
-                         &c.gen_temp, &c.gen_aux})
+                         &c.d_ctrl, &c.d_match, &c.d_husband, &c.d_prank, &c.d_qcnt, &c.d_qoff, &c.d_qlist,
+                         &c.gen_keys_a, &c.gen_keys_b, &c.gen_seg, &c.gen_temp, &c.gen_aux})
       b->release();
     for (auto &e : c.ev)
       if (e) cudaEventDestroy(e);
@@ -532,8 +624,7 @@ int smp_b200_solve(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w, i
     if (cudaEventRecord(c.ev[kEvCheckBegin], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
     // The checker reuses the solve's rank matrix; only a perfect instance
     // (which skipped the inversion) builds it here.
-    if (!rc) rc = c.rank_bytes == 2 ? enqueue_invert<uint16_t>(c, c.pref_w, c.d_rank.as<uint16_t>(), kInvertIfPerfect)
-                                    : enqueue_invert<int32_t>(c, c.pref_w, c.d_rank.as<int32_t>(), kInvertIfPerfect);
+    if (!rc) rc = enqueue_invert_any(c, kGateNoRank);
     if (!rc) rc = enqueue_check(c, c.d_match.as<int32_t>());
     if (!rc && cudaEventRecord(c.ev[kEvCheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
   }
@@ -582,7 +673,7 @@ int smp_b200_invert(smp_ctx *ctx, const int32_t *pref_w, int32_t n, int32_t *ran
   if (cudaMemcpyAsync(c.d_ctrl.ptr, c.h_ctrl, sizeof(Control), cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
     return c.fail_cuda("control reset");
   if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
-  rc = enqueue_invert<int32_t>(c, src, dst, kInvertAlways);
+  rc = enqueue_invert<int32_t>(c, src, dst, kGateAlways);
   if (rc) return rc;
   if (cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
   if (!(flags & SMP_F_DEVICE_PTRS)) {
@@ -622,8 +713,7 @@ int smp_b200_check(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w, i
   rc = c.d_rank.ensure(static_cast<size_t>(n) * n * c.rank_bytes);
   if (rc) return rc;
   if (cudaEventRecord(c.ev[kEvCheckBegin], c.stream) != cudaSuccess) return c.fail_cuda("event");
-  rc = c.rank_bytes == 2 ? enqueue_invert<uint16_t>(c, c.pref_w, c.d_rank.as<uint16_t>(), kInvertAlways)
-                         : enqueue_invert<int32_t>(c, c.pref_w, c.d_rank.as<int32_t>(), kInvertAlways);
+  rc = enqueue_invert_any(c, kGateAlways);
   if (!rc) rc = enqueue_check(c, dmatch);
   if (rc) return rc;
   if (cudaEventRecord(c.ev[kEvCheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");

@@ -1,43 +1,68 @@
 // solve_kernels.cuh -- the sm_100a kernels of one Gale-Shapley solve.
 //
-//   k_precheck   distinct first choices?   (SmpEngineBamboo::IsPerfect,
-//                                           include/smp/smp_engine_bamboo.h:25-33)
-//   k_invert     rank[w][pref_w[w][r]] = r (F9RankMatrixInitKernel,
-//                                           src/smp/kernel.cu:672-686)
-//   k_prefix     per-man (woman, rank) pairs for the first K choices, the
-//                part of the reference's PR matrix (kernel.cu:688-709) that a
-//                solve actually reads
-//   k_bulk       proposals on every SM      (La3F9CoreKernel, kernel.cu:633-670)
-//   k_tail       the last chains in one CTA (MonitorProceture + LAProcedure,
-//                                           src/smp/smp_engine_bamboo.cu:197-287)
-//   k_match      match[m] = w               (SmpEngineBamboo::PostProc,
-//                                           smp_engine_bamboo.cu:289-306)
-//   k_check_*    stability checker (no counterpart in the reference)
+//   k_precheck    distinct first choices; picks the mode  (SmpEngineBamboo::IsPerfect,
+//                                                          include/smp/smp_engine_bamboo.h:25-33)
+//   k_invert      rank[w][pref_w[w][r]] = r              (F9RankMatrixInitKernel,
+//                                                          src/smp/kernel.cu:672-686)
+//   k_prefix      per-man (woman, rank) pairs for the first K choices, gathered
+//                 from the rank matrix: the part of the reference's PR matrix
+//                 (kernel.cu:688-709) that a solve reads
+//   k_q*          the same prefix answered straight from pref_w rows, without
+//                 a rank matrix (query mode)
+//   k_bulk        proposals on every SM                  (La3F9CoreKernel, kernel.cu:633-670)
+//   k_tail        the last chains in one CTA             (MonitorProceture + LAProcedure,
+//                                                          src/smp/smp_engine_bamboo.cu:197-287)
+//   k_match       match[m] = w                           (SmpEngineBamboo::PostProc,
+//                                                          smp_engine_bamboo.cu:289-306)
+//   k_check_*     stability checker (no counterpart in the reference)
 //
-// Layouts (all row-major, 64-bit offsets):
+// Layouts (row-major, 64-bit offsets):
 //   pref_m, pref_w  int32 [n][n]
 //   rank            RankT [n][n], RankT = uint16_t for n <= 65535, else int32
-//   prefix          uint32 [n][K] = woman << 16 | rank of the man for her
+//   prefix          uint32 [n][K] = woman << 16 | her rank of the man
+//   qoff, qlist     query index: the (man << 16 | position) pairs naming woman
+//                   w among a man's first K choices are qlist[qoff[w] .. qoff[w+1])
 //   bid             u64 [n] (see common.cuh)
+//
+// Every kernel opens with a gate (below) read from the control block, so the
+// host enqueues the whole pipeline once and the device decides which parts
+// run: no host round trip inside a solve.
 #pragma once
 
 #include "common.cuh"
 
 namespace smpb200 {
 
-// When an inversion kernel runs, given the precheck's verdict.
-constexpr int kInvertAlways = 0;
-constexpr int kInvertUnlessPerfect = 1;  // the solve's own inversion
-constexpr int kInvertIfPerfect = 2;      // the checker after a perfect solve
+// ---------------------------------------------------------------------------
+// Gates.
+// ---------------------------------------------------------------------------
+enum Gate : int {
+  kGateAlways = 0,
+  kGateMain = 1,       // round 0 of a solve: not perfect, no error seen
+  kGateModeRank = 2,   // round 0 in rank mode
+  kGateModeQuery = 3,  // round 0 in query mode
+  kGateRetry = 4,      // the rank-mode round after a query-mode abort
+  kGateIfPerfect = 5,  // the checker after a perfect solve (needs its own inversion)
+  kGateNoRank = 6,     // the checker after a solve that built no rank matrix
+};
 
-__device__ __forceinline__ bool invert_skipped(int mode, const Control *ctrl) {
-  if (mode == kInvertAlways) return false;
-  const int perfect = ld_volatile_s32(&ctrl->perfect);
-  return mode == kInvertUnlessPerfect ? perfect != 0 : perfect == 0;
+__device__ __forceinline__ bool gate_open(int gate, const Control *c) {
+  if (gate == kGateAlways) return true;
+  const int perfect = ld_volatile_s32(&c->perfect);
+  if (gate == kGateIfPerfect) return perfect != 0;
+  if (gate == kGateNoRank) return perfect != 0 || ld_volatile_s32(&c->mode) == kModeQuery;
+  if (perfect || ld_volatile_s32(&c->status)) return false;
+  switch (gate) {
+    case kGateMain: return true;
+    case kGateModeRank: return ld_volatile_s32(&c->mode) == kModeRank;
+    case kGateModeQuery: return ld_volatile_s32(&c->mode) == kModeQuery;
+    case kGateRetry: return ld_volatile_s32(&c->retry) != 0;
+    default: return false;
+  }
 }
 
-// Unset marker of a rank-matrix slot during inversion: never a valid rank
-// (uint16 ranks are < n <= 65535; int32 ranks are >= 0).
+// Unset marker of a rank slot during inversion: never a valid rank (uint16
+// ranks are < n <= 65535; int32 ranks are >= 0).
 template <typename RankT>
 __device__ __forceinline__ RankT rank_unset();
 template <>
@@ -45,31 +70,71 @@ __device__ __forceinline__ uint16_t rank_unset<uint16_t>() { return 0xFFFFu; }
 template <>
 __device__ __forceinline__ int32_t rank_unset<int32_t>() { return -1; }
 
+// Does a 16-byte chunk of ranks hold an unset slot?
+template <typename RankT>
+__device__ __forceinline__ bool any_unset(uint4 v);
+template <>
+__device__ __forceinline__ bool any_unset<uint16_t>(uint4 v) {
+  return (__vcmpeq2(v.x, 0xFFFFFFFFu) | __vcmpeq2(v.y, 0xFFFFFFFFu) | __vcmpeq2(v.z, 0xFFFFFFFFu) |
+          __vcmpeq2(v.w, 0xFFFFFFFFu)) != 0;
+}
+template <>
+__device__ __forceinline__ bool any_unset<int32_t>(uint4 v) {
+  return v.x == 0xFFFFFFFFu || v.y == 0xFFFFFFFFu || v.z == 0xFFFFFFFFu || v.w == 0xFFFFFFFFu;
+}
+
 // ---------------------------------------------------------------------------
-// Precheck: ctrl->perfect stays 1 iff the n first choices are distinct.
-// seen: ceil(n/32) zeroed words.
+// Precheck.  Marks each man's first choice in an n-bit bitmap (seen, zeroed
+// by the host).  The last block to finish counts the distinct first choices
+// and decides: perfect (all distinct, if allowed) and the mode -- query mode
+// when at least a quarter of the first choices are distinct (proposals spread
+// over the women, so each man stays within his prefix), rank mode otherwise
+// (a few women draw most first proposals and men go deep into their lists).
 // ---------------------------------------------------------------------------
-__global__ void k_precheck(const int32_t *__restrict__ pref_m, int n,
-                           uint32_t *__restrict__ seen, Control *ctrl) {
+__global__ void __launch_bounds__(256) k_precheck(const int32_t *__restrict__ pref_m, int n,
+                                                  uint32_t *__restrict__ seen, Control *ctrl) {
   const int stride = gridDim.x * blockDim.x;
   for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += stride) {
     const int w = __ldg(pref_m + static_cast<size_t>(m) * n);
     if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) {
       report(ctrl, kStatusInvalidInput, w);
-      ctrl->perfect = 0;
       continue;
     }
-    const uint32_t bit = 1u << (w & 31);
-    if (atomicOr(seen + (w >> 5), bit) & bit) ctrl->perfect = 0;
+    atomicOr(seen + (w >> 5), 1u << (w & 31));
+  }
+  __shared__ int s_last;
+  __shared__ int s_count;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&ctrl->blocks_done, 1) == static_cast<int>(gridDim.x) - 1;
+    s_count = 0;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  int count = 0;
+  const int words = (n + 31) >> 5;
+  for (int i = threadIdx.x; i < words; i += blockDim.x) count += __popc(__ldcg(seen + i));
+  atomicAdd(&s_count, count);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int distinct = s_count;
+    ctrl->distinct = distinct;
+    ctrl->perfect = (ctrl->allow_perfect && distinct == n && ctrl->status == 0) ? 1 : 0;
+    ctrl->mode = (ctrl->allow_query && 4ll * distinct >= n) ? kModeQuery : kModeRank;
   }
 }
 
 // ---------------------------------------------------------------------------
-// Inversion.  One CTA inverts one row of pref_w at a time: the row streams in
-// with 16-byte loads, each (r, m) is scattered into a shared-memory copy of
-// the rank row, and the finished row streams out with 16-byte stores.  A
-// slot still unset after the scatter means the row was not a permutation.
-// Dynamic shared memory: n * sizeof(RankT) bytes, 16-byte aligned.
+// Row inversion in shared memory.  One CTA handles one row of pref_w at a
+// time: 16-byte streaming loads, each (r, m) scattered into the shared rank
+// row, then (k_invert) the row streams out with 16-byte stores, or
+// (k_qinvert) the queries of that woman are answered from it.  The shared
+// row is offset so that its 16-byte chunks line up with the 16-byte chunks of
+// the destination row, which keeps both the shared reads and the global
+// stores vectorised and free of bank conflicts.  A slot still unset after
+// the scatter means the row was not a permutation.
 // ---------------------------------------------------------------------------
 template <typename RankT>
 __device__ __forceinline__ void scatter_one(RankT *srow, int m, int r, int n, bool &bad) {
@@ -88,73 +153,77 @@ __device__ __forceinline__ void scatter4(RankT *srow, int4 q, int r, int n, bool
   scatter_one(srow, q.w, r + 3, n, bad);
 }
 
+// Shared bytes for one row with the alignment offset.
 template <typename RankT>
-__global__ void __launch_bounds__(512) k_invert(const int32_t *__restrict__ pref_w,
-                                                RankT *__restrict__ rank, int n,
-                                                Control *ctrl, int mode) {
-  if (invert_skipped(mode, ctrl)) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  RankT *srow = reinterpret_cast<RankT *>(smem_raw);
-  constexpr int kPerVec = 16 / sizeof(RankT);  // ranks per 16-byte store
+__host__ __device__ constexpr size_t row_smem_bytes(int n) {
+  return ((static_cast<size_t>(n) + 2 * (16 / sizeof(RankT))) * sizeof(RankT) + 15) & ~static_cast<size_t>(15);
+}
+
+// Clears the chunks [0, chunks) of sbuf, then streams row `row` of pref_w in
+// and scatters it into srow (= sbuf + offset).  Ends with __syncthreads.
+template <typename RankT>
+__device__ __forceinline__ void load_row(const int32_t *__restrict__ row, RankT *sbuf, RankT *srow, int chunks,
+                                         int n, bool &bad) {
   const int tid = threadIdx.x;
   const int nthr = blockDim.x;
+  uint4 *s4 = reinterpret_cast<uint4 *>(sbuf);
+  const uint4 fill = make_uint4(~0u, ~0u, ~0u, ~0u);
+  for (int i = tid; i < chunks; i += nthr) s4[i] = fill;
+  __syncthreads();
+  const int head = min(n, static_cast<int>(((16u - (reinterpret_cast<uintptr_t>(row) & 15u)) & 15u) >> 2));
+  if (tid < head) scatter_one(srow, __ldcs(row + tid), tid, n, bad);
+  const int nq = (n - head) >> 2;
+  const int4 *rq = reinterpret_cast<const int4 *>(row + head);
+  int i = tid;
+  for (; i + 3 * nthr < nq; i += 4 * nthr) {
+    const int4 a = __ldcs(rq + i);
+    const int4 b = __ldcs(rq + i + nthr);
+    const int4 c = __ldcs(rq + i + 2 * nthr);
+    const int4 d = __ldcs(rq + i + 3 * nthr);
+    scatter4(srow, a, head + 4 * i, n, bad);
+    scatter4(srow, b, head + 4 * (i + nthr), n, bad);
+    scatter4(srow, c, head + 4 * (i + 2 * nthr), n, bad);
+    scatter4(srow, d, head + 4 * (i + 3 * nthr), n, bad);
+  }
+  for (; i < nq; i += nthr) scatter4(srow, __ldcs(rq + i), head + 4 * i, n, bad);
+  for (int t = head + 4 * nq + tid; t < n; t += nthr) scatter_one(srow, __ldcs(row + t), t, n, bad);
+  __syncthreads();
+}
+
+template <typename RankT>
+__global__ void __launch_bounds__(512) k_invert(const int32_t *__restrict__ pref_w, RankT *__restrict__ rank,
+                                                int n, Control *ctrl, int gate) {
+  if (!gate_open(gate, ctrl)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RankT *sbuf = reinterpret_cast<RankT *>(smem_raw);
+  constexpr int kPerVec = 16 / sizeof(RankT);
+  const RankT unset = rank_unset<RankT>();
   bool bad = false;
-
   for (int w = blockIdx.x; w < n; w += gridDim.x) {
-    // 1. mark every slot unset (16-byte shared stores)
-    {
-      uint4 *s4 = reinterpret_cast<uint4 *>(srow);
-      const int nvec = (n + kPerVec - 1) / kPerVec;
-      const uint4 fill = make_uint4(~0u, ~0u, ~0u, ~0u);
-      for (int i = tid; i < nvec; i += nthr) s4[i] = fill;
-    }
-    __syncthreads();
-
-    // 2. stream the preference row in and scatter ranks
-    const int32_t *row = pref_w + static_cast<size_t>(w) * n;
-    const int head = min(n, static_cast<int>(((16u - (reinterpret_cast<uintptr_t>(row) & 15u)) & 15u) >> 2));
-    if (tid < head) scatter_one(srow, __ldcs(row + tid), tid, n, bad);
-    const int nq = (n - head) >> 2;
-    const int4 *rq = reinterpret_cast<const int4 *>(row + head);
-    int i = tid;
-    for (; i + 3 * nthr < nq; i += 4 * nthr) {
-      const int4 a = __ldcs(rq + i);
-      const int4 b = __ldcs(rq + i + nthr);
-      const int4 c = __ldcs(rq + i + 2 * nthr);
-      const int4 d = __ldcs(rq + i + 3 * nthr);
-      scatter4(srow, a, head + 4 * i, n, bad);
-      scatter4(srow, b, head + 4 * (i + nthr), n, bad);
-      scatter4(srow, c, head + 4 * (i + 2 * nthr), n, bad);
-      scatter4(srow, d, head + 4 * (i + 3 * nthr), n, bad);
-    }
-    for (; i < nq; i += nthr) scatter4(srow, __ldcs(rq + i), head + 4 * i, n, bad);
-    for (int t = head + 4 * nq + tid; t < n; t += nthr) scatter_one(srow, __ldcs(row + t), t, n, bad);
-    __syncthreads();
-
-    // 3. stream the rank row out, checking for unset slots
     RankT *out = rank + static_cast<size_t>(w) * n;
-    const RankT unset = rank_unset<RankT>();
-    const int ohead = min(n, static_cast<int>(((16u - (reinterpret_cast<uintptr_t>(out) & 15u)) & 15u) / sizeof(RankT)));
-    for (int t = tid; t < ohead; t += nthr) {
-      const RankT v = srow[t];
-      bad |= (v == unset);
-      __stcs(out + t, v);
-    }
-    const int nv = (n - ohead) / kPerVec;
-    uint4 *o4 = reinterpret_cast<uint4 *>(out + ohead);
-    for (int v = tid; v < nv; v += nthr) {
-      RankT vals[kPerVec];
+    const int pre = static_cast<int>((reinterpret_cast<uintptr_t>(out) & 15u) / sizeof(RankT));
+    const int chunks = (pre + n + kPerVec - 1) / kPerVec;
+    load_row(pref_w + static_cast<size_t>(w) * n, sbuf, sbuf + pre, chunks, n, bad);
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(sbuf);
+    uint4 *o4 = reinterpret_cast<uint4 *>(reinterpret_cast<uintptr_t>(out) -
+                                          static_cast<uintptr_t>(pre) * sizeof(RankT));
+    for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
+      const uint4 v = s4[c];
+      const int first = c * kPerVec - pre;  // row element in the chunk's first slot
+      if (first >= 0 && first + kPerVec <= n) {
+        bad |= any_unset<RankT>(v);
+        __stcs(o4 + c, v);
+      } else {
+        const RankT *vals = reinterpret_cast<const RankT *>(&v);
 #pragma unroll
-      for (int k = 0; k < kPerVec; ++k) {
-        vals[k] = srow[ohead + v * kPerVec + k];
-        bad |= (vals[k] == unset);
+        for (int k = 0; k < kPerVec; ++k) {
+          const int e = first + k;
+          if (e >= 0 && e < n) {
+            bad |= (vals[k] == unset);
+            __stcs(out + e, vals[k]);
+          }
+        }
       }
-      __stcs(o4 + v, *reinterpret_cast<const uint4 *>(vals));
-    }
-    for (int t = ohead + nv * kPerVec + tid; t < n; t += nthr) {
-      const RankT v = srow[t];
-      bad |= (v == unset);
-      __stcs(out + t, v);
     }
     __syncthreads();
   }
@@ -163,9 +232,9 @@ __global__ void __launch_bounds__(512) k_invert(const int32_t *__restrict__ pref
 
 // Inversion for rows that do not fit in shared memory: scatter straight to
 // global memory, then verify rank[w][pref_w[w][r]] == r in a second pass.
-__global__ void k_invert_global(const int32_t *__restrict__ pref_w, int32_t *__restrict__ rank,
-                                int n, Control *ctrl, int mode) {
-  if (invert_skipped(mode, ctrl)) return;
+__global__ void k_invert_global(const int32_t *__restrict__ pref_w, int32_t *__restrict__ rank, int n,
+                                Control *ctrl, int gate) {
+  if (!gate_open(gate, ctrl)) return;
   const size_t total = static_cast<size_t>(n) * n;
   const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
   for (size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
@@ -179,27 +248,24 @@ __global__ void k_invert_global(const int32_t *__restrict__ pref_w, int32_t *__r
     }
   }
 }
-__global__ void k_invert_verify(const int32_t *__restrict__ pref_w, const int32_t *__restrict__ rank,
-                                int n, Control *ctrl, int mode) {
-  if (invert_skipped(mode, ctrl)) return;
+__global__ void k_invert_verify(const int32_t *__restrict__ pref_w, const int32_t *__restrict__ rank, int n,
+                                Control *ctrl, int gate) {
+  if (!gate_open(gate, ctrl)) return;
   const size_t total = static_cast<size_t>(n) * n;
   const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
   for (size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
     const int w = static_cast<int>(t / n);
     const int r = static_cast<int>(t - static_cast<size_t>(w) * n);
     const int m = pref_w[t];
-    if (static_cast<unsigned>(m) >= static_cast<unsigned>(n) ||
-        rank[static_cast<size_t>(w) * n + m] != r) {
+    if (static_cast<unsigned>(m) >= static_cast<unsigned>(n) || rank[static_cast<size_t>(w) * n + m] != r)
       report(ctrl, kStatusInvalidInput, m);
-    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // Full validation (SMP_F_VALIDATE): every row of a preference matrix is a
 // permutation of 0..n-1.  One CTA per row at a time with an n-bit shared
-// bitmap; a value out of range or seen twice is reported.
-// Dynamic shared memory: ceil(n/32) * 4 bytes.
+// bitmap.  Dynamic shared memory: ceil(n/32) * 4 bytes.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(512) k_validate_rows(const int32_t *__restrict__ pref, int n, Control *ctrl) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -230,13 +296,13 @@ __global__ void __launch_bounds__(512) k_validate_rows(const int32_t *__restrict
 }
 
 // ---------------------------------------------------------------------------
-// Prefix gather: prefix[m][r] = pref_m[m][r] << 16 | rank[pref_m[m][r]][m]
-// for r < K (uint16 ranks only).  An out-of-range woman is reported and her
-// entry set to 0xFFFFFFFF.
+// Prefix gather (rank mode): prefix[m][r] = w << 16 | rank[w][m] for
+// w = pref_m[m][r], r < K.  An out-of-range woman is reported and her entry
+// set to 0xFFFFFFFF.
 // ---------------------------------------------------------------------------
 __global__ void k_prefix(const int32_t *__restrict__ pref_m, const uint16_t *__restrict__ rank,
-                         uint32_t *__restrict__ prefix, int n, int K, Control *ctrl) {
-  if (ld_volatile_s32(&ctrl->perfect) || ld_volatile_s32(&ctrl->status)) return;
+                         uint32_t *__restrict__ prefix, int n, int K, Control *ctrl, int gate) {
+  if (!gate_open(gate, ctrl)) return;
   const size_t total = static_cast<size_t>(n) * K;
   const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
   for (size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
@@ -254,117 +320,272 @@ __global__ void k_prefix(const int32_t *__restrict__ pref_m, const uint16_t *__r
 }
 
 // ---------------------------------------------------------------------------
-// Window of 32 consecutive choices of one man, one per lane: lane l looks at
-// position pos + l.  Returns false (and reports) for an out-of-range woman.
+// Query mode.  The prefix needs rank_w(m) only for the n*K pairs (w, m) with
+// w among m's first K choices.  k_qcount / k_qscan / k_qscatter bucket those
+// pairs by woman (a counting sort of n*K entries); k_qinvert then streams each
+// woman's row once, inverts it in shared memory and answers her bucket.  The
+// rank matrix is never written: pref_w is read once and nothing n^2-sized is
+// stored.  qcnt is zeroed by the host.
+// ---------------------------------------------------------------------------
+__global__ void k_qcount(const int32_t *__restrict__ pref_m, int n, int K, int32_t *__restrict__ qcnt,
+                         Control *ctrl) {
+  if (!gate_open(kGateModeQuery, ctrl)) return;
+  const size_t total = static_cast<size_t>(n) * K;
+  const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+  for (size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const int m = static_cast<int>(t / K);
+    const int r = static_cast<int>(t - static_cast<size_t>(m) * K);
+    const int w = __ldg(pref_m + static_cast<size_t>(m) * n + r);
+    if (static_cast<unsigned>(w) < static_cast<unsigned>(n)) {
+      atomicAdd(qcnt + w, 1);
+    } else {
+      report(ctrl, kStatusInvalidInput, w);
+    }
+  }
+}
+
+// One CTA of 1024 threads: exclusive scan of qcnt into qoff[0..n], then
+// qcnt is zeroed for use as the fill counter.
+__global__ void __launch_bounds__(1024) k_qscan(int32_t *__restrict__ qcnt, int32_t *__restrict__ qoff, int n,
+                                                Control *ctrl) {
+  if (!gate_open(kGateModeQuery, ctrl)) return;
+  __shared__ int s_warp[32];
+  const int tid = threadIdx.x;
+  const int per = (n + blockDim.x - 1) / blockDim.x;
+  const int lo = min(n, tid * per), hi = min(n, lo + per);
+  int sum = 0;
+  for (int i = lo; i < hi; ++i) sum += qcnt[i];
+  // block-wide exclusive scan of the per-thread sums
+  const int lane = tid & 31, warp = tid >> 5;
+  int x = sum;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int y = __shfl_up_sync(kFullMask, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int v = lane < static_cast<int>(blockDim.x >> 5) ? s_warp[lane] : 0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(kFullMask, v, off);
+      if (lane >= off) v += y;
+    }
+    s_warp[lane] = v;
+  }
+  __syncthreads();
+  int run = x - sum + (warp > 0 ? s_warp[warp - 1] : 0);
+  for (int i = lo; i < hi; ++i) {
+    const int c = qcnt[i];
+    qoff[i] = run;
+    run += c;
+    qcnt[i] = 0;
+  }
+  if (tid == static_cast<int>(blockDim.x) - 1) qoff[n] = run;
+}
+
+__global__ void k_qscatter(const int32_t *__restrict__ pref_m, int n, int K, const int32_t *__restrict__ qoff,
+                           int32_t *__restrict__ qfill, uint32_t *__restrict__ qlist, Control *ctrl) {
+  if (!gate_open(kGateModeQuery, ctrl)) return;
+  const size_t total = static_cast<size_t>(n) * K;
+  const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+  for (size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const int m = static_cast<int>(t / K);
+    const int r = static_cast<int>(t - static_cast<size_t>(m) * K);
+    const int w = __ldg(pref_m + static_cast<size_t>(m) * n + r);
+    if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) continue;  // reported by k_qcount
+    const int slot = qoff[w] + atomicAdd(qfill + w, 1);
+    qlist[slot] = (static_cast<uint32_t>(m) << 16) | static_cast<uint32_t>(r);
+  }
+}
+
+__global__ void __launch_bounds__(512) k_qinvert(const int32_t *__restrict__ pref_w, int n, int K,
+                                                 const int32_t *__restrict__ qoff,
+                                                 const uint32_t *__restrict__ qlist,
+                                                 uint32_t *__restrict__ prefix, Control *ctrl) {
+  if (!gate_open(kGateModeQuery, ctrl)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint16_t *srow = reinterpret_cast<uint16_t *>(smem_raw);
+  const int chunks = (n + 7) / 8;
+  bool bad = false;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    load_row(pref_w + static_cast<size_t>(w) * n, srow, srow, chunks, n, bad);
+    // validation: every slot written
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(srow);
+    for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
+      uint4 v = s4[c];
+      const int tailn = n - c * 8;
+      if (tailn < 8) {  // slots past n keep the fill value; mask them out
+        const auto keep = [tailn](uint32_t x, int half) -> uint32_t {
+          return x & ((half < tailn ? 0x0000FFFFu : 0u) | (half + 1 < tailn ? 0xFFFF0000u : 0u));
+        };
+        v.x = keep(v.x, 0);
+        v.y = keep(v.y, 2);
+        v.z = keep(v.z, 4);
+        v.w = keep(v.w, 6);
+      }
+      bad |= any_unset<uint16_t>(v);
+    }
+    const int q0 = qoff[w], q1 = qoff[w + 1];
+    for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+      const uint32_t e = qlist[q];
+      const uint32_t m = e >> 16, r = e & 0xFFFFu;
+      prefix[static_cast<size_t>(m) * K + r] = (static_cast<uint32_t>(w) << 16) | srow[m];
+    }
+    __syncthreads();
+  }
+  if (bad) report(ctrl, kStatusInvalidInput, -1);
+}
+
+// ---------------------------------------------------------------------------
+// One choice of a man: his r-th woman and her rank of him.
+//   0  ok
+//   1  beyond the prefix while in query mode (rank unknown)
+//   2  out-of-range woman (reported by the caller)
 // ---------------------------------------------------------------------------
 template <typename RankT>
-__device__ __forceinline__ bool load_choice(const int32_t *__restrict__ pref_m,
-                                            const RankT *__restrict__ rank,
-                                            const uint32_t *__restrict__ prefix, int K, int n,
-                                            int m, int r, int &w, uint32_t &rk) {
+__device__ __forceinline__ int load_choice(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank,
+                                           const uint32_t *__restrict__ prefix, int K, int n, bool query, int m,
+                                           int r, int &w, uint32_t &rk) {
   if (r < K) {
     const uint32_t e = __ldg(prefix + static_cast<size_t>(m) * K + r);
     w = static_cast<int>(e >> 16);
     rk = e & 0xFFFFu;
-    return e != 0xFFFFFFFFu;
+    return e == 0xFFFFFFFFu ? 2 : 0;
   }
+  if (query) return 1;
   w = __ldg(pref_m + static_cast<size_t>(m) * n + r);
-  if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) return false;
+  if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) return 2;
   rk = static_cast<uint32_t>(__ldg(rank + static_cast<size_t>(w) * n + m));
-  return true;
+  return 0;
 }
 
+// Look-ahead: a warp examines up to kMaxSub windows of 32 choices per step
+// (a template parameter: 1, 2, 4 or 8).
+
 // ---------------------------------------------------------------------------
-// Bulk proposals.  Each warp carries one free man at a time.  It looks at
-// his next 32 choices at once; every woman whose current partner she ranks
-// above him would reject him, so those proposals are settled by one relaxed
-// read of her bid word.  For the first remaining candidate the warp proposes
-// with a 64-bit atomicMin.  If accepted and she had a partner, the warp
-// continues with the displaced man from the position stored in the returned
-// word; if she was free, the number of free women drops and the warp takes a
-// man who has not proposed yet.  Once no more than tail_threshold women are
-// free, warps hand their man to the tail queue and stop.
+// Bulk proposals.  Each warp carries one free man at a time and looks at his
+// next S*32 choices at once (S = 1 for a man just taken up, doubling up to
+// kMaxSub while whole windows reject him).  Every woman whose current partner she
+// ranks above him would reject him, so those proposals are settled by one
+// relaxed read of her bid word; for the first remaining candidate the warp
+// proposes with a 64-bit atomicMin.  If accepted and she had a partner, the
+// warp continues with the displaced man from the position stored in the
+// returned word; if she was free, the count of free women drops and the warp
+// takes a man who has not proposed yet.  Once no more than tail_threshold
+// women are free, warps hand their man to the tail queue and stop.  In query
+// mode a man whose next proposal lies beyond his prefix stops the solve for
+// the rank-mode retry round.
+// round 0: gate Main; round 1: gate Retry (rank mode).
 // ---------------------------------------------------------------------------
-template <typename RankT>
-__global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m,
-                                              const RankT *__restrict__ rank,
+template <typename RankT, int kMaxSub>
+__global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank,
                                               const uint32_t *__restrict__ prefix, int K,
-                                              unsigned long long *bid, Control *ctrl,
-                                              int2 *tail_queue, int n, int tail_threshold) {
-  if (ld_volatile_s32(&ctrl->perfect) || ld_volatile_s32(&ctrl->status)) return;
+                                              unsigned long long *bid, Control *ctrl, int2 *tail_queue, int n,
+                                              int tail_threshold, int round) {
+  if (!gate_open(round == 0 ? kGateMain : kGateRetry, ctrl)) return;
+  const bool query = round == 0 && ld_volatile_s32(&ctrl->mode) == kModeQuery;
   const int lane = threadIdx.x & 31;
-  int m = -1, pos = 0;
+  int m = -1, pos = 0, S = 1;
   unsigned long long settled = 0;  // proposals this warp decided (lane 0's copy is used)
   unsigned int hops = 0;           // proposals this warp saw accepted
   for (;;) {
-    int free_now = 0;
     if (m < 0) {
       int v = n;
-      if (lane == 0) {
-        if (tail_threshold <= 0 || ld_relaxed_s32(&ctrl->free_count) > tail_threshold)
-          v = atomicAdd(&ctrl->next_man, 1);
-      }
+      if (lane == 0 && ld_relaxed_s32(&ctrl->free_count) > tail_threshold) v = atomicAdd(&ctrl->next_man, 1);
       v = __shfl_sync(kFullMask, v, 0);
       if (v >= n) break;
       m = v;
       pos = 0;
+      S = 1;
     }
-    if (tail_threshold > 0 && lane == 0) free_now = ld_relaxed_s32(&ctrl->free_count);
+    int free_now = 0;
+    if (lane == 0) free_now = ld_relaxed_s32(&ctrl->free_count);
 
-    const int r = pos + lane;
-    const bool valid = r < n;
-    int w = 0;
-    uint32_t rk = 0xFFFFFFFFu;
-    bool ok = true;
-    if (valid) ok = load_choice(pref_m, rank, prefix, K, n, m, r, w, rk);
-    const unsigned long long cur = (valid && ok) ? ld_relaxed_u64(bid + w) : 0ull;
-
-    if (tail_threshold > 0) {
-      free_now = __shfl_sync(kFullMask, free_now, 0);
-      if (free_now <= tail_threshold) {
-        if (lane == 0) {
-          const int q = atomicAdd(&ctrl->tail_count, 1);
-          tail_queue[q] = make_int2(m, pos);
+    int w[kMaxSub], st[kMaxSub];
+    uint32_t rk[kMaxSub];
+    unsigned long long cur[kMaxSub];
+#pragma unroll
+    for (int s = 0; s < kMaxSub; ++s) {
+      st[s] = 3;  // past the end of the list / unused
+      cur[s] = 0;
+      rk[s] = 0xFFFFFFFFu;
+      w[s] = 0;
+      if (s < S) {
+        const int r = pos + 32 * s + lane;
+        if (r < n) {
+          st[s] = load_choice(pref_m, rank, prefix, K, n, query, m, r, w[s], rk[s]);
+          if (st[s] == 0) cur[s] = ld_relaxed_u64(bid + w[s]);
         }
-        break;
       }
     }
-    const unsigned badmask = __ballot_sync(kFullMask, valid && !ok);
-    if (badmask) {
-      if (lane == __ffs(badmask) - 1) report(ctrl, kStatusInvalidInput, w);
+    free_now = __shfl_sync(kFullMask, free_now, 0);
+    if (free_now <= tail_threshold) {  // hand over (also how a retry stops everyone)
+      // A round-0 abort drops the men: the retry round starts from scratch.
+      if (lane == 0 && !(round == 0 && ld_volatile_s32(&ctrl->retry))) {
+        const int q = atomicAdd(&ctrl->tail_count, 1);
+        tail_queue[q] = make_int2(m, pos);
+      }
       break;
     }
 
-    unsigned cand = __ballot_sync(kFullMask, valid && rk < bid_rank(cur));
-    bool moved = false;
-    while (cand) {
-      const int j = __ffs(cand) - 1;
-      unsigned long long old = 0;
-      if (lane == j) old = atomicMin(bid + w, pack_bid(rk, static_cast<uint32_t>(m), static_cast<uint32_t>(r)));
-      old = __shfl_sync(kFullMask, old, j);
-      const uint32_t rkj = __shfl_sync(kFullMask, rk, j);
-      if (bid_rank(old) > rkj) {  // accepted: she was free or held a worse man
-        settled += j + 1;
-        hops++;
-        if (old == kFree) {
-          if (lane == 0) atomicSub(&ctrl->free_count, 1);
-          m = -1;
+    bool moved = false, stop = false;
+#pragma unroll
+    for (int s = 0; s < kMaxSub; ++s) {
+      if (s < S && !moved && !stop) {
+        const unsigned badm = __ballot_sync(kFullMask, st[s] == 2);
+        if (badm) {
+          if (lane == __ffs(badm) - 1) report(ctrl, kStatusInvalidInput, w[s]);
+          stop = true;
         } else {
-          m = static_cast<int>(bid_man(old));
-          pos = static_cast<int>(bid_pos(old)) + 1;
+          const unsigned beyond = __ballot_sync(kFullMask, st[s] == 1);
+          const unsigned before = beyond ? ((1u << (__ffs(beyond) - 1)) - 1u) : kFullMask;
+          unsigned cand = __ballot_sync(kFullMask, st[s] == 0 && rk[s] < bid_rank(cur[s])) & before;
+          while (cand) {
+            const int j = __ffs(cand) - 1;
+            unsigned long long old = 0;
+            if (lane == j)
+              old = atomicMin(bid + w[s], pack_bid(rk[s], static_cast<uint32_t>(m),
+                                                   static_cast<uint32_t>(pos + 32 * s + j)));
+            old = __shfl_sync(kFullMask, old, j);
+            const uint32_t rkj = __shfl_sync(kFullMask, rk[s], j);
+            if (bid_rank(old) > rkj) {  // accepted: she was free or held a worse man
+              settled += 32 * s + j + 1;
+              hops++;
+              if (old == kFree) {
+                if (lane == 0) atomicSub(&ctrl->free_count, 1);
+                m = -1;
+              } else {
+                m = static_cast<int>(bid_man(old));
+                pos = static_cast<int>(bid_pos(old)) + 1;
+                S = 1;
+              }
+              moved = true;
+              break;
+            }
+            cand &= cand - 1;  // someone better got there first
+          }
+          if (!moved && beyond) {  // query mode ran out of prefix: retry in rank mode
+            if (lane == 0) {
+              atomicExch(&ctrl->retry, 1);
+              atomicExch(&ctrl->free_count, -(1 << 30));
+            }
+            stop = true;
+          }
         }
-        moved = true;
-        break;
       }
-      cand &= cand - 1;  // someone better got there first
     }
+    if (stop) break;
     if (!moved) {
-      settled += min(32, n - pos);
-      pos += 32;
+      const int scanned = 32 * S;
+      settled += min(scanned, n - pos);
+      pos += scanned;
       if (pos >= n) {  // rejected by every woman: the lists are not permutations
         if (lane == 0) report(ctrl, kStatusInvalidInput, m);
         break;
       }
+      S = min(2 * S, kMaxSub);
     }
   }
   if (lane == 0 && settled) {
@@ -373,15 +594,13 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
   }
 }
 
-// Largest n whose tail state (4-byte bid + 2-byte position per person) fits
-// in one CTA's shared memory next to the tail's small bookkeeping.
-constexpr int kTailSmemBytesMax = 227 * 1024;
+// Shared memory of the tail: 4-byte bid and 2-byte position per person.
 __host__ __device__ constexpr size_t tail_smem_bytes(int n) {
   return static_cast<size_t>(n) * 4 + ((static_cast<size_t>(n) * 2 + 15) & ~static_cast<size_t>(15)) + 64;
 }
 
-__device__ __forceinline__ void write_perfect(const int32_t *__restrict__ pref_m, int32_t *match,
-                                              int n, Control *ctrl) {
+__device__ __forceinline__ void write_perfect(const int32_t *__restrict__ pref_m, int32_t *match, int n,
+                                              Control *ctrl) {
   const int stride = gridDim.x * blockDim.x;
   for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += stride)
     match[m] = __ldg(pref_m + static_cast<size_t>(m) * n);
@@ -390,29 +609,34 @@ __device__ __forceinline__ void write_perfect(const int32_t *__restrict__ pref_m
 
 // ---------------------------------------------------------------------------
 // Tail.  One CTA of 32 warps.  The bid words move into shared memory as
-// rank << 16 | man (4 bytes; n <= 65535), and each man's position in his
-// own list into a shared 2-byte array, written before every proposal and
-// published by the acquire-release shared atomicMin.  Warps take men from the
-// bulk kernel's queue and from the men that never proposed, and follow their
-// chains exactly as k_bulk does, but every bid read and atomic stays inside
-// the SM.  At the end the CTA writes match[] and the proposal count.
+// rank << 16 | man (n <= 65535), and each man's position in his own list
+// into a shared 2-byte array, written before every proposal and published by
+// the acquire-release shared atomicMin.  Warps take men from the bulk
+// kernel's queue and from the men that never proposed, and follow their
+// chains as k_bulk does, with every bid read and atomic inside the SM.  At
+// the end the CTA writes match[] and the proposal count.  In query mode a man
+// beyond his prefix sets the retry flag and every warp stops.
+// round 0: gate Main (and no retry pending); round 1: gate Retry.
 // ---------------------------------------------------------------------------
-template <typename RankT>
+template <typename RankT, int kMaxSub>
 __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pref_m,
                                                   const RankT *__restrict__ rank,
                                                   const uint32_t *__restrict__ prefix, int K,
-                                                  const unsigned long long *__restrict__ bid,
-                                                  Control *ctrl, const int2 *__restrict__ tail_queue,
-                                                  int32_t *__restrict__ match, int n) {
-  if (ld_volatile_s32(&ctrl->perfect)) {
+                                                  const unsigned long long *__restrict__ bid, Control *ctrl,
+                                                  const int2 *__restrict__ tail_queue,
+                                                  int32_t *__restrict__ match, int n, int round) {
+  if (round == 0 && ld_volatile_s32(&ctrl->perfect)) {
     write_perfect(pref_m, match, n, ctrl);
     return;
   }
-  if (ld_volatile_s32(&ctrl->status)) return;
+  if (!gate_open(round == 0 ? kGateMain : kGateRetry, ctrl)) return;
+  if (round == 0 && ld_volatile_s32(&ctrl->retry)) return;
+  const bool query = round == 0 && ld_volatile_s32(&ctrl->mode) == kModeQuery;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint32_t *sbid = reinterpret_cast<uint32_t *>(smem_raw);
   uint16_t *spos = reinterpret_cast<uint16_t *>(smem_raw + static_cast<size_t>(n) * 4);
   __shared__ int s_next;
+  __shared__ int s_abort;
   __shared__ unsigned long long s_props;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -432,12 +656,13 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
   }
   if (tid == 0) {
     s_next = 0;
+    s_abort = 0;
     s_props = 0;
     ctrl->tail_men = total;
   }
   __syncthreads();
 
-  int m = -1, pos = 0;
+  int m = -1, pos = 0, S = 1;
   unsigned long long settled = 0;
   unsigned int hops = 0;
   for (;;) {
@@ -454,54 +679,82 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
         m = first_unstarted + (i - queued);
         pos = 0;
       }
+      S = 1;
     }
-    const int r = pos + lane;
-    const bool valid = r < n;
-    int w = 0;
-    uint32_t rk = 0xFFFFFFFFu;
-    bool ok = true;
-    if (valid) ok = load_choice(pref_m, rank, prefix, K, n, m, r, w, rk);
-    const unsigned badmask = __ballot_sync(kFullMask, valid && !ok);
-    if (badmask) {
-      if (lane == __ffs(badmask) - 1) report(ctrl, kStatusInvalidInput, w);
-      break;
-    }
-    const uint32_t cur = valid ? lds_relaxed_u32(sbid + w) : 0u;
-    unsigned cand = __ballot_sync(kFullMask, valid && rk < (cur >> 16));
-    bool moved = false;
-    while (cand) {
-      const int j = __ffs(cand) - 1;
-      uint32_t old = 0;
-      int next_pos = 0;
-      if (lane == j) {
-        spos[m] = static_cast<uint16_t>(r);
-        old = atom_min_acq_rel_shared(sbid + w, (rk << 16) | static_cast<uint32_t>(m));
-        if ((old >> 16) > rk && old != 0xFFFFFFFFu) next_pos = spos[old & 0xFFFFu] + 1;
+    int w[kMaxSub], st[kMaxSub];
+    uint32_t rk[kMaxSub];
+#pragma unroll
+    for (int s = 0; s < kMaxSub; ++s) {
+      st[s] = 3;
+      rk[s] = 0xFFFFFFFFu;
+      w[s] = 0;
+      if (s < S) {
+        const int r = pos + 32 * s + lane;
+        if (r < n) st[s] = load_choice(pref_m, rank, prefix, K, n, query, m, r, w[s], rk[s]);
       }
-      old = __shfl_sync(kFullMask, old, j);
-      next_pos = __shfl_sync(kFullMask, next_pos, j);
-      const uint32_t rkj = __shfl_sync(kFullMask, rk, j);
-      if ((old >> 16) > rkj) {
-        settled += j + 1;
-        hops++;
-        if (old == 0xFFFFFFFFu) {
-          m = -1;
+    }
+    if (*reinterpret_cast<volatile int *>(&s_abort)) break;
+
+    bool moved = false, stop = false;
+#pragma unroll
+    for (int s = 0; s < kMaxSub; ++s) {
+      if (s < S && !moved && !stop) {
+        const unsigned badm = __ballot_sync(kFullMask, st[s] == 2);
+        if (badm) {
+          if (lane == __ffs(badm) - 1) report(ctrl, kStatusInvalidInput, w[s]);
+          stop = true;
         } else {
-          m = static_cast<int>(old & 0xFFFFu);
-          pos = next_pos;
+          const uint32_t cur = st[s] == 0 ? lds_relaxed_u32(sbid + w[s]) : 0u;
+          const unsigned beyond = __ballot_sync(kFullMask, st[s] == 1);
+          const unsigned before = beyond ? ((1u << (__ffs(beyond) - 1)) - 1u) : kFullMask;
+          unsigned cand = __ballot_sync(kFullMask, st[s] == 0 && rk[s] < (cur >> 16)) & before;
+          while (cand) {
+            const int j = __ffs(cand) - 1;
+            uint32_t old = 0;
+            int next_pos = 0;
+            if (lane == j) {
+              spos[m] = static_cast<uint16_t>(pos + 32 * s + j);
+              old = atom_min_acq_rel_shared(sbid + w[s], (rk[s] << 16) | static_cast<uint32_t>(m));
+              if ((old >> 16) > rk[s] && old != 0xFFFFFFFFu) next_pos = spos[old & 0xFFFFu] + 1;
+            }
+            old = __shfl_sync(kFullMask, old, j);
+            next_pos = __shfl_sync(kFullMask, next_pos, j);
+            const uint32_t rkj = __shfl_sync(kFullMask, rk[s], j);
+            if ((old >> 16) > rkj) {
+              settled += 32 * s + j + 1;
+              hops++;
+              if (old == 0xFFFFFFFFu) {
+                m = -1;
+              } else {
+                m = static_cast<int>(old & 0xFFFFu);
+                pos = next_pos;
+                S = 1;
+              }
+              moved = true;
+              break;
+            }
+            cand &= cand - 1;
+          }
+          if (!moved && beyond) {
+            if (lane == 0) {
+              s_abort = 1;
+              atomicExch(&ctrl->retry, 1);
+            }
+            stop = true;
+          }
         }
-        moved = true;
-        break;
       }
-      cand &= cand - 1;
     }
+    if (stop) break;
     if (!moved) {
-      settled += min(32, n - pos);
-      pos += 32;
+      const int scanned = 32 * S;
+      settled += min(scanned, n - pos);
+      pos += scanned;
       if (pos >= n) {
         if (lane == 0) report(ctrl, kStatusInvalidInput, m);
         break;
       }
+      S = min(2 * S, kMaxSub);
     }
   }
   if (lane == 0 && settled) {
@@ -509,6 +762,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
     atomicAdd(&ctrl->tail_hops, hops);
   }
   __syncthreads();
+  if (s_abort || ld_volatile_s32(&ctrl->status)) return;
 
   unsigned long long props = 0;
   for (int w = tid; w < n; w += blockDim.x) {
@@ -525,6 +779,26 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
   if (lane == 0) atomicAdd(&s_props, props);
   __syncthreads();
   if (tid == 0) ctrl->proposals = s_props;
+}
+
+// ---------------------------------------------------------------------------
+// Start of the rank-mode retry round: every woman free again, counters reset.
+// One CTA.
+// ---------------------------------------------------------------------------
+__global__ void k_retry_reset(unsigned long long *bid, int n, Control *ctrl) {
+  if (!gate_open(kGateRetry, ctrl)) return;
+  for (int w = threadIdx.x; w < n; w += blockDim.x) bid[w] = kFree;
+  if (threadIdx.x == 0) {
+    ctrl->mode = kModeRank;
+    ctrl->next_man = 0;
+    ctrl->free_count = n;
+    ctrl->tail_count = 0;
+    ctrl->tail_men = 0;
+    ctrl->bulk_proposals = 0;
+    ctrl->tail_proposals = 0;
+    ctrl->bulk_hops = 0;
+    ctrl->tail_hops = 0;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -562,8 +836,7 @@ __global__ void k_match(const int32_t *__restrict__ pref_m, const unsigned long 
 //     is a blocking pair if she ranks him above her husband.  Also sums the
 //     proposal count (position of the wife + 1).
 // ---------------------------------------------------------------------------
-__global__ void k_check_husband(const int32_t *__restrict__ match, int32_t *husband, int n,
-                                Control *ctrl) {
+__global__ void k_check_husband(const int32_t *__restrict__ match, int32_t *husband, int n, Control *ctrl) {
   const int stride = gridDim.x * blockDim.x;
   for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += stride) {
     const int w = match[m];
@@ -589,8 +862,8 @@ __global__ void k_check_prank(const int32_t *__restrict__ husband, const RankT *
 
 template <typename RankT>
 __global__ void k_check_scan(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank,
-                             const int32_t *__restrict__ match, const int32_t *__restrict__ prank,
-                             int n, Control *ctrl) {
+                             const int32_t *__restrict__ match, const int32_t *__restrict__ prank, int n,
+                             Control *ctrl) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   unsigned long long blocking = 0, props = 0;
