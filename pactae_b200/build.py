@@ -1,6 +1,6 @@
 """Build recipe for libsmp_b200.so (sm_100a) and the CPU oracle.
 
-``python -m pactae_b200.build`` compiles the CUDA sources in
+``python pactae_b200/build.py`` compiles the CUDA sources in
 ``pactae_b200/csrc`` with nvcc straight into ``pactae_b200/libsmp_b200.so``
 (in-tree, so the built library travels with the working tree).  Every source
 is compiled for ``sm_100a`` only.  A rebuild happens only when a source or
@@ -32,7 +32,7 @@ NVCC_FLAGS = [
     "-Xptxas", "-warn-spills",
 ]
 
-SOURCES = ["smp_b200.cu", "generate.cu"]
+SOURCES = ["smp_b200.cu", "generate.cu", "static_solve.cu"]
 
 
 def _nvcc() -> str:

@@ -21,6 +21,17 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "slow: full-size (n=30000) cases")
 
 
+def load_build_recipe():
+    """pactae_b200/build.py, loaded by path: importing the package would load
+    the (possibly stale) library before it is rebuilt."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("pactae_b200_build", ROOT / "pactae_b200" / "build.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def pytest_sessionstart(session):
     # Build the oracle (test infrastructure) and the CUDA library in-tree
     # before any test module imports them.
@@ -28,9 +39,7 @@ def pytest_sessionstart(session):
 
     if not oracle.ORACLE_LIB.exists():
         oracle.build()
-    from pactae_b200 import build as pbuild
-
-    pbuild.build()
+    load_build_recipe().build()
 
 
 def load_cases() -> list[dict]:

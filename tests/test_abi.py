@@ -43,8 +43,9 @@ def test_library_exports_every_declared_symbol():
 
 def test_library_is_built_for_sm100a():
     # The build recipe compiles for sm_100a only.
-    from pactae_b200 import build as pbuild
+    from conftest import load_build_recipe
 
+    pbuild = load_build_recipe()
     assert pbuild.ARCH_FLAGS == ["-gencode", "arch=compute_100a,code=sm_100a"]
     assert _lib.LIB_PATH.exists()
 
