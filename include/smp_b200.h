@@ -170,6 +170,26 @@ SMP_B200_API int smp_b200_check(smp_ctx *ctx, const int32_t *pref_m, const int32
                    int32_t n, const int32_t *match, uint32_t flags,
                    int64_t *blocking_pairs, int64_t *proposals);
 
+/* Largest n smp_b200_solve_static accepts. */
+#define SMP_B200_STATIC_MAX_N 1024
+
+/* A whole solve that allocates nothing.  No counterpart in the reference:
+ * it exists for callers that cannot allocate device memory when they need a
+ * matching -- an application whose device memory is already held by its own
+ * caching allocator, a process under a per-process device-memory limit, or a
+ * loop that must not stall on cudaMalloc/cudaFree.  pref_m, pref_w and
+ * match_out are device pointers on the current device; stream is a
+ * cudaStream_t (NULL = the legacy default stream); proposals may be NULL.
+ * All scratch lives in one file-scope device array of 2 MiB + 256 bytes that
+ * every GPU loading the library keeps until exit, so n is limited to
+ * SMP_B200_STATIC_MAX_N (larger n returns SMP_ERR_UNSUPPORTED before
+ * anything runs).  The first call on a device looks up the array's device
+ * address, so make it before any stream capture.  Every call shares the
+ * array: calls that overlap on the GPU race, so order them on one stream.
+ * Returns after the work has finished. */
+SMP_B200_API int smp_b200_solve_static(const int32_t *pref_m, const int32_t *pref_w, int32_t n,
+                                       int32_t *match_out, int64_t *proposals, void *stream);
+
 /* Seeded workload generator.  salt separates instances of a batch; param is
  * sigma*1e4 (CORRELATED) or the group size (GROUPED).  Writes both lists,
  * drawn from counter-based Philox4x32-10 streams (pactae_b200/csrc/generate.cu

@@ -23,6 +23,7 @@ SMP_ERR_NOT_READY = 7
 SMP_ERR_UNSUPPORTED = 8
 
 SMP_B200_MAX_N = 1048575
+SMP_B200_STATIC_MAX_N = 1024
 
 SMP_F_DEVICE_PTRS = 0x1
 SMP_F_CHECK = 0x2
@@ -53,6 +54,7 @@ ABI_SYMBOLS = (
     "smp_b200_invert",
     "smp_b200_check",
     "smp_b200_generate",
+    "smp_b200_solve_static",
 )
 
 
@@ -120,6 +122,7 @@ _SIGNATURES = {
     "smp_b200_check": (ctypes.c_int, [_P, _P, _P, _I32, _P, _U32, ctypes.POINTER(ctypes.c_int64),
                                       ctypes.POINTER(ctypes.c_int64)]),
     "smp_b200_generate": (ctypes.c_int, [_P, _I32, _I32, _U64, _U32, _I32, _P, _P, _U32]),
+    "smp_b200_solve_static": (ctypes.c_int, [_P, _P, _I32, _P, ctypes.POINTER(ctypes.c_int64), _P]),
 }
 
 
