@@ -32,8 +32,8 @@
  *                        FindStableMatching (include/utils/types.h:44).
  *   smp_b200_generate    GenerateWorkload (include/utils/generate_workloads_flat.h:250-280),
  *                        seeded.
- *   smp_b200_solve_batch many SmpEngineExecutor runs
- *                        (benchmark/smp_engine_exec.h:6-32) in one launch.
+ *   smp_b200_batch_*     many SmpEngineExecutor runs
+ *   smp_b200_solve_batch (benchmark/smp_engine_exec.h:6-32) in one launch.
  *   smp_b200_submit / smp_b200_poll
  *                        no counterpart (serving loop on top of the solver).
  *
@@ -169,6 +169,65 @@ SMP_B200_API int smp_b200_invert(smp_ctx *ctx, const int32_t *pref_w, int32_t n,
 SMP_B200_API int smp_b200_check(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w,
                    int32_t n, const int32_t *match, uint32_t flags,
                    int64_t *blocking_pairs, int64_t *proposals);
+
+/* ------------------------------------------------------------------------ */
+/* Batches: many independent instances in one persistent launch.            */
+/* ------------------------------------------------------------------------ */
+
+/* One instance of a batch.  All pointers are device pointers on the
+ * context's device; status and proposals are filled in by a run. */
+typedef struct smp_instance {
+  const int32_t *pref_m;   /* n*n int32, row-major                          */
+  const int32_t *pref_w;   /* n*n int32, row-major                          */
+  int32_t *match;          /* n int32: match[m] = w                          */
+  int32_t n;               /* 1 .. SMP_B200_BATCH_MAX_N                      */
+  int32_t status;          /* out: smp_status of this instance               */
+  int64_t proposals;       /* out: Gale-Shapley proposals                    */
+} smp_instance;
+
+/* Largest instance a batch accepts (each CTA keeps one instance's bids and
+ * positions in shared memory). */
+#define SMP_B200_BATCH_MAX_N 16384
+
+typedef struct smp_batch_cfg {
+  int32_t block_threads;   /* threads per CTA (128..512); 0 = auto           */
+  int32_t ctas_per_sm;     /* resident CTAs per SM; 0 = auto                 */
+  int32_t window;          /* look-ahead choices per warp step; 0 = auto     */
+  int32_t use_graph;       /* 1 (default, also 0 here) = replay a captured   */
+                           /* CUDA graph; -1 = plain stream launch           */
+  int32_t reserved[4];
+} smp_batch_cfg;
+
+typedef struct smp_batch_stats {
+  int32_t instances;       /* instances in the batch                         */
+  int32_t failed;          /* instances whose status is not SMP_OK           */
+  int64_t proposals;       /* sum over the instances                         */
+  float ms;                /* device time of the run (CUDA events)           */
+  int32_t launches;        /* kernel launches the run made                   */
+} smp_batch_stats;
+
+typedef struct smp_batch smp_batch;
+
+/* Prepares a batch: uploads the instance table (sorted largest first for
+ * the work queue), sizes per-CTA scratch for the largest n and captures the
+ * batched step as a CUDA graph.  The table is copied; the device buffers it
+ * points to must stay valid while the batch is used.  cfg may be NULL. */
+SMP_B200_API int smp_b200_batch_create(smp_ctx *ctx, const smp_instance *inst, int32_t count,
+                                       const smp_batch_cfg *cfg, smp_batch **out);
+/* One batched run: every instance solved by the persistent kernel.
+ * results (may be NULL) receives the table with status and proposals. */
+SMP_B200_API int smp_b200_batch_run(smp_batch *batch, smp_instance *results, smp_batch_stats *st);
+/* The same kernel launched once per instance (the per-instance baseline). */
+SMP_B200_API int smp_b200_batch_run_plain(smp_batch *batch, smp_instance *results, smp_batch_stats *st);
+SMP_B200_API void smp_b200_batch_destroy(smp_batch *batch);
+/* create + run + destroy; the status and proposals of inst[] are filled in. */
+SMP_B200_API int smp_b200_solve_batch(smp_ctx *ctx, smp_instance *inst, int32_t count, const smp_batch_cfg *cfg,
+                                      smp_batch_stats *st);
+/* Size and kind of instance b of a seeded mix: n = floor(n_lo * (n_hi/n_lo)^u)
+ * (log-uniform) and kind uniform / congested / correlated, from the same
+ * Philox stream as smp_b200_generate.  Host only. */
+SMP_B200_API void smp_b200_batch_instance(uint64_t seed, uint32_t b, int32_t n_lo, int32_t n_hi, int32_t *n_out,
+                                          int32_t *kind_out);
 
 /* Largest n smp_b200_solve_static accepts. */
 #define SMP_B200_STATIC_MAX_N 1024

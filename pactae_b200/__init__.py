@@ -43,11 +43,14 @@ from ._lib import (  # noqa: F401  (re-exported constants)
     SMP_GEN_UNIFORM,
     SMP_OK,
     lib,
+    smp_batch_cfg,
+    smp_batch_stats,
     smp_cfg,
+    smp_instance,
     smp_stats,
 )
 
-__all__ = ["Context", "SmpError", "SmpObj", "SmpEngineB200", "version"]
+__all__ = ["Batch", "Context", "SmpError", "SmpObj", "SmpEngineB200", "batch_instance", "version"]
 
 
 class SmpError(RuntimeError):
@@ -230,6 +233,12 @@ class Context:
         _check(rc, "smp_b200_check")
         return int(bp.value), int(props.value)
 
+    def generate_into(self, kind: int, n: int, seed: int, pref_m_ptr: int, pref_w_ptr: int, salt: int = 0,
+                      param: int = 0) -> None:
+        """Seeded instance written to caller-owned device memory (n*n int32 each)."""
+        _check(lib.smp_b200_generate(self.handle, kind, n, seed, salt, param, ctypes.c_void_p(pref_m_ptr),
+                                     ctypes.c_void_p(pref_w_ptr), SMP_F_DEVICE_PTRS), "smp_b200_generate")
+
     def generate(self, kind: int, n: int, seed: int, salt: int = 0, param: int = 0,
                  device: bool = True) -> tuple[Any, Any]:
         """Seeded instance (pref_m, pref_w): CUDA tensors if device, else numpy."""
@@ -248,6 +257,82 @@ class Context:
         _check(lib.smp_b200_generate(self.handle, kind, n, seed, salt, param, _ptr(pm), _ptr(pw), 0),
                "smp_b200_generate")
         return pm, pw
+
+
+def batch_instance(seed: int, b: int, n_lo: int, n_hi: int) -> tuple[int, int]:
+    """(n, kind) of instance b of a seeded mix (log-uniform n in [n_lo, n_hi],
+    kind uniform / congested / correlated)."""
+    n = ctypes.c_int32()
+    kind = ctypes.c_int32()
+    lib.smp_b200_batch_instance(seed, b, n_lo, n_hi, ctypes.byref(n), ctypes.byref(kind))
+    return n.value, kind.value
+
+
+class Batch:
+    """A batch of independent instances solved by one persistent launch
+    (smp_b200_batch_*).  instances: sequence of (pref_m, pref_w, match) CUDA
+    tensors (int32, n*n / n*n / n) on the context's device; they must stay
+    alive while the batch is used."""
+
+    def __init__(self, ctx: Context, instances, block_threads: int = 0, ctas_per_sm: int = 0, window: int = 0,
+                 use_graph: bool = True):
+        self.ctx = ctx
+        self._keep = list(instances)
+        count = len(self._keep)
+        table = (smp_instance * count)()
+        for i, (pm, pw, mt) in enumerate(self._keep):
+            n = int(mt.numel())
+            if pm.numel() != n * n or pw.numel() != n * n:
+                raise ValueError(f"instance {i}: lists must hold n*n values")
+            table[i].pref_m = pm.data_ptr()
+            table[i].pref_w = pw.data_ptr()
+            table[i].match = mt.data_ptr()
+            table[i].n = n
+        self._table = table
+        cfg = smp_batch_cfg()
+        cfg.block_threads = block_threads
+        cfg.ctas_per_sm = ctas_per_sm
+        cfg.window = window
+        cfg.use_graph = 1 if use_graph else -1
+        handle = ctypes.c_void_p()
+        import torch
+
+        torch.cuda.synchronize()
+        _check(lib.smp_b200_batch_create(ctx.handle, table, count, ctypes.byref(cfg), ctypes.byref(handle)),
+               "smp_b200_batch_create")
+        self._h = handle
+        self.count = count
+
+    def _run(self, fn) -> tuple[list[int], list[int], dict]:
+        results = (smp_instance * self.count)()
+        st = smp_batch_stats()
+        _check(fn(self._h, results, ctypes.byref(st)), "smp_b200_batch_run")
+        return [r.status for r in results], [r.proposals for r in results], st.as_dict()
+
+    def run(self) -> tuple[list[int], list[int], dict]:
+        """Batched persistent launch: (statuses, proposals, stats)."""
+        return self._run(lib.smp_b200_batch_run)
+
+    def run_plain(self) -> tuple[list[int], list[int], dict]:
+        """The same kernel launched once per instance."""
+        return self._run(lib.smp_b200_batch_run_plain)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.smp_b200_batch_destroy(self._h)
+        self._h = None
+
+    def __enter__(self) -> "Batch":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class SmpObj:

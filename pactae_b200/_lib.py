@@ -24,6 +24,7 @@ SMP_ERR_UNSUPPORTED = 8
 
 SMP_B200_MAX_N = 1048575
 SMP_B200_STATIC_MAX_N = 1024
+SMP_B200_BATCH_MAX_N = 16384
 
 SMP_F_DEVICE_PTRS = 0x1
 SMP_F_CHECK = 0x2
@@ -55,6 +56,12 @@ ABI_SYMBOLS = (
     "smp_b200_check",
     "smp_b200_generate",
     "smp_b200_solve_static",
+    "smp_b200_batch_create",
+    "smp_b200_batch_run",
+    "smp_b200_batch_run_plain",
+    "smp_b200_batch_destroy",
+    "smp_b200_solve_batch",
+    "smp_b200_batch_instance",
 )
 
 
@@ -101,6 +108,40 @@ class smp_stats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("reserved")}
 
 
+class smp_instance(ctypes.Structure):
+    _fields_ = [
+        ("pref_m", ctypes.c_void_p),
+        ("pref_w", ctypes.c_void_p),
+        ("match", ctypes.c_void_p),
+        ("n", ctypes.c_int32),
+        ("status", ctypes.c_int32),
+        ("proposals", ctypes.c_int64),
+    ]
+
+
+class smp_batch_cfg(ctypes.Structure):
+    _fields_ = [
+        ("block_threads", ctypes.c_int32),
+        ("ctas_per_sm", ctypes.c_int32),
+        ("window", ctypes.c_int32),
+        ("use_graph", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
+    ]
+
+
+class smp_batch_stats(ctypes.Structure):
+    _fields_ = [
+        ("instances", ctypes.c_int32),
+        ("failed", ctypes.c_int32),
+        ("proposals", ctypes.c_int64),
+        ("ms", ctypes.c_float),
+        ("launches", ctypes.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
 _U32 = ctypes.c_uint32
@@ -123,6 +164,14 @@ _SIGNATURES = {
                                       ctypes.POINTER(ctypes.c_int64)]),
     "smp_b200_generate": (ctypes.c_int, [_P, _I32, _I32, _U64, _U32, _I32, _P, _P, _U32]),
     "smp_b200_solve_static": (ctypes.c_int, [_P, _P, _I32, _P, ctypes.POINTER(ctypes.c_int64), _P]),
+    "smp_b200_batch_create": (ctypes.c_int, [_P, ctypes.POINTER(smp_instance), _I32, ctypes.POINTER(smp_batch_cfg),
+                                             ctypes.POINTER(_P)]),
+    "smp_b200_batch_run": (ctypes.c_int, [_P, ctypes.POINTER(smp_instance), ctypes.POINTER(smp_batch_stats)]),
+    "smp_b200_batch_run_plain": (ctypes.c_int, [_P, ctypes.POINTER(smp_instance), ctypes.POINTER(smp_batch_stats)]),
+    "smp_b200_batch_destroy": (None, [_P]),
+    "smp_b200_solve_batch": (ctypes.c_int, [_P, ctypes.POINTER(smp_instance), _I32, ctypes.POINTER(smp_batch_cfg),
+                                            ctypes.POINTER(smp_batch_stats)]),
+    "smp_b200_batch_instance": (None, [_U64, _U32, _I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
 }
 
 

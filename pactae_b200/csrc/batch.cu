@@ -1,0 +1,294 @@
+// batch.cu -- the batch ABI: many instances in one persistent launch,
+// captured as a CUDA graph, and the one-launch-per-instance baseline.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "batch_kernels.cuh"
+#include "common.cuh"
+#include "internal.h"
+
+using namespace smpb200;
+
+static_assert(sizeof(smp_instance) == sizeof(BatchInstance), "smp_instance mirrors the device table row");
+static_assert(offsetof(smp_instance, n) == offsetof(BatchInstance, n), "layout");
+static_assert(offsetof(smp_instance, proposals) == offsetof(BatchInstance, proposals), "layout");
+
+struct smp_batch {
+  smp_ctx *ctx = nullptr;
+  int count = 0;
+  int max_n = 0;
+  int block = 512;
+  int grid = 0;
+  int subs = 8;
+  bool use_graph = true;
+  size_t slab_elems = 0;
+  size_t smem = 0;
+  DeviceBuf d_table, d_order, d_queue, d_slabs;
+  std::vector<int32_t> order;
+  smp_instance *h_table = nullptr;  // pinned copy for results
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+// Total scratch the rank slabs of one batch may take.
+constexpr size_t kSlabBudget = 24ull << 30;
+
+int subs_for_window(int window) {
+  if (window <= 0) return 8;
+  if (window <= 32) return 1;
+  if (window <= 64) return 2;
+  if (window <= 128) return 4;
+  return 8;
+}
+
+template <int kSub>
+int launch_batch_t(smp_batch &b, cudaStream_t s, int grid, const int32_t *order, int count, int dynamic) {
+  k_batch<kSub><<<grid, b.block, b.smem, s>>>(b.d_table.as<BatchInstance>(), order, count, b.d_queue.as<int>(),
+                                              b.d_slabs.as<uint16_t>(), b.slab_elems, b.max_n, dynamic);
+  return b.ctx->c.check_launch("k_batch");
+}
+
+// Dynamic shared memory of the chosen kernel (set before any capture).
+int set_batch_attribute(smp_batch &b) {
+  cudaError_t e;
+  switch (b.subs) {
+    case 1: e = cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b.smem)); break;
+    case 2: e = cudaFuncSetAttribute(k_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b.smem)); break;
+    case 4: e = cudaFuncSetAttribute(k_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b.smem)); break;
+    default: e = cudaFuncSetAttribute(k_batch<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b.smem)); break;
+  }
+  return e == cudaSuccess ? SMP_OK : b.ctx->c.fail_cuda("k_batch smem attribute");
+}
+
+int launch_batch(smp_batch &b, cudaStream_t s, int grid, const int32_t *order, int count, int dynamic) {
+  switch (b.subs) {
+    case 1: return launch_batch_t<1>(b, s, grid, order, count, dynamic);
+    case 2: return launch_batch_t<2>(b, s, grid, order, count, dynamic);
+    case 4: return launch_batch_t<4>(b, s, grid, order, count, dynamic);
+    default: return launch_batch_t<8>(b, s, grid, order, count, dynamic);
+  }
+}
+
+// The batched step: reset the queue, run the persistent kernel, copy the
+// table (statuses, proposals) back to pinned host memory.
+int enqueue_step(smp_batch &b, cudaStream_t s) {
+  if (cudaMemsetAsync(b.d_queue.ptr, 0, sizeof(int), s) != cudaSuccess) return b.ctx->c.fail_cuda("queue reset");
+  int rc = launch_batch(b, s, b.grid, b.d_order.as<int32_t>(), b.count, 1);
+  if (rc) return rc;
+  if (cudaMemcpyAsync(b.h_table, b.d_table.ptr, sizeof(smp_instance) * b.count, cudaMemcpyDeviceToHost, s) !=
+      cudaSuccess)
+    return b.ctx->c.fail_cuda("table readback");
+  return SMP_OK;
+}
+
+void fill_batch_stats(const smp_batch &b, smp_instance *results, smp_batch_stats *st, float ms, int launches) {
+  int failed = 0;
+  long long props = 0;
+  for (int i = 0; i < b.count; ++i) {
+    if (b.h_table[i].status != SMP_OK) failed++;
+    props += b.h_table[i].proposals;
+  }
+  if (results) std::memcpy(results, b.h_table, sizeof(smp_instance) * b.count);
+  if (st) {
+    *st = smp_batch_stats{};
+    st->instances = b.count;
+    st->failed = failed;
+    st->proposals = props;
+    st->ms = ms;
+    st->launches = launches;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int smp_b200_batch_create(smp_ctx *ctx, const smp_instance *inst, int32_t count, const smp_batch_cfg *cfg,
+                          smp_batch **out) {
+  if (!ctx || !inst || count <= 0 || !out) return SMP_ERR_INVALID_ARG;
+  *out = nullptr;
+  Ctx &c = ctx->c;
+  DeviceGuard g(c.device);
+  auto *b = new (std::nothrow) smp_batch();
+  if (!b) return SMP_ERR_OOM;
+  b->ctx = ctx;
+  b->count = count;
+  for (int i = 0; i < count; ++i) {
+    if (!inst[i].pref_m || !inst[i].pref_w || !inst[i].match || inst[i].n <= 0 || inst[i].n > SMP_B200_BATCH_MAX_N) {
+      delete b;
+      c.last_error = "batch: null pointer or n out of range";
+      return SMP_ERR_INVALID_ARG;
+    }
+    b->max_n = std::max(b->max_n, static_cast<int>(inst[i].n));
+  }
+  // Work queue order: largest instances first (longest-processing-time).
+  b->order.resize(count);
+  std::iota(b->order.begin(), b->order.end(), 0);
+  std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return inst[x].n > inst[y].n; });
+
+  b->block = (cfg && cfg->block_threads > 0) ? std::min(512, std::max(64, cfg->block_threads / 32 * 32)) : 512;
+  b->subs = subs_for_window(cfg ? cfg->window : 0);
+  b->use_graph = !(cfg && cfg->use_graph < 0);
+  b->smem = batch_smem_bytes(b->max_n);
+  if (b->smem > c.smem_optin) {
+    delete b;
+    return SMP_ERR_UNSUPPORTED;
+  }
+  int per_sm = (cfg && cfg->ctas_per_sm > 0) ? cfg->ctas_per_sm : 0;
+  if (per_sm == 0) {
+    // as many as fit (shared memory and threads), at most 4
+    const int by_threads = 2048 / b->block;
+    const int by_smem = static_cast<int>(std::max<size_t>(1, (c.smem_optin + 1024) / (b->smem + 1024)));
+    per_sm = std::max(1, std::min(4, std::min(by_threads, by_smem)));
+  }
+  b->slab_elems = static_cast<size_t>(b->max_n) * b->max_n;
+  const size_t slab_bytes = b->slab_elems * sizeof(uint16_t);
+  const int by_budget = static_cast<int>(std::max<size_t>(1, kSlabBudget / slab_bytes));
+  b->grid = std::max(1, std::min({c.sm_count * per_sm, by_budget, count}));
+
+  int rc = b->d_table.ensure(sizeof(BatchInstance) * count);
+  if (!rc) rc = b->d_order.ensure(sizeof(int32_t) * count);
+  if (!rc) rc = b->d_queue.ensure(sizeof(int));
+  if (!rc) rc = b->d_slabs.ensure(slab_bytes * b->grid);
+  if (!rc && cudaMallocHost(reinterpret_cast<void **>(&b->h_table), sizeof(smp_instance) * count) != cudaSuccess) {
+    cudaGetLastError();
+    rc = SMP_ERR_OOM;
+  }
+  if (!rc && (cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)) rc = SMP_ERR_CUDA;
+  if (rc) {
+    smp_b200_batch_destroy(b);
+    return rc;
+  }
+  std::memcpy(b->h_table, inst, sizeof(smp_instance) * count);
+  for (int i = 0; i < count; ++i) {
+    b->h_table[i].status = SMP_ERR_NOT_READY;
+    b->h_table[i].proposals = 0;
+  }
+  if (cudaMemcpyAsync(b->d_table.ptr, b->h_table, sizeof(smp_instance) * count, cudaMemcpyHostToDevice, c.stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(b->d_order.ptr, b->order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, c.stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(c.stream) != cudaSuccess) {
+    c.fail_cuda("batch upload");
+    smp_b200_batch_destroy(b);
+    return SMP_ERR_CUDA;
+  }
+  rc = set_batch_attribute(*b);
+  if (rc) {
+    smp_b200_batch_destroy(b);
+    return rc;
+  }
+  if (b->use_graph) {
+    // Capture the batched step once; every run replays it.
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      c.fail_cuda("batch capture");
+      smp_b200_batch_destroy(b);
+      return SMP_ERR_CUDA;
+    }
+    rc = enqueue_step(*b, c.stream);
+    const cudaError_t end = cudaStreamEndCapture(c.stream, &graph);
+    if (rc || end != cudaSuccess || cudaGraphInstantiate(&b->exec, graph, 0) != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (!rc) rc = c.fail_cuda("batch graph");
+      smp_b200_batch_destroy(b);
+      return rc;
+    }
+    cudaGraphDestroy(graph);
+  }
+  *out = b;
+  return SMP_OK;
+}
+
+int smp_b200_batch_run(smp_batch *b, smp_instance *results, smp_batch_stats *st) {
+  if (!b) return SMP_ERR_INVALID_ARG;
+  Ctx &c = b->ctx->c;
+  DeviceGuard g(c.device);
+  if (cudaEventRecord(b->ev0, c.stream) != cudaSuccess) return c.fail_cuda("event");
+  int rc = SMP_OK;
+  if (b->exec) {
+    if (cudaGraphLaunch(b->exec, c.stream) != cudaSuccess) rc = c.fail_cuda("batch graph launch");
+  } else {
+    rc = enqueue_step(*b, c.stream);
+  }
+  if (rc) return rc;
+  if (cudaEventRecord(b->ev1, c.stream) != cudaSuccess) return c.fail_cuda("event");
+  rc = c.sync("batch run");
+  if (rc) return rc;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+  fill_batch_stats(*b, results, st, ms, 1);
+  return SMP_OK;
+}
+
+int smp_b200_batch_run_plain(smp_batch *b, smp_instance *results, smp_batch_stats *st) {
+  if (!b) return SMP_ERR_INVALID_ARG;
+  Ctx &c = b->ctx->c;
+  DeviceGuard g(c.device);
+  if (cudaEventRecord(b->ev0, c.stream) != cudaSuccess) return c.fail_cuda("event");
+  // One launch per instance: grid of one CTA, its own instance, no queue.
+  for (int k = 0; k < b->count; ++k) {
+    const int rc = launch_batch(*b, c.stream, 1, b->d_order.as<int32_t>() + k, 1, 0);
+    if (rc) return rc;
+  }
+  if (cudaMemcpyAsync(b->h_table, b->d_table.ptr, sizeof(smp_instance) * b->count, cudaMemcpyDeviceToHost,
+                      c.stream) != cudaSuccess)
+    return c.fail_cuda("table readback");
+  if (cudaEventRecord(b->ev1, c.stream) != cudaSuccess) return c.fail_cuda("event");
+  const int rc = c.sync("batch run plain");
+  if (rc) return rc;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+  fill_batch_stats(*b, results, st, ms, b->count);
+  return SMP_OK;
+}
+
+void smp_b200_batch_destroy(smp_batch *b) {
+  if (!b) return;
+  {
+    DeviceGuard g(b->ctx->c.device);
+    cudaStreamSynchronize(b->ctx->c.stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->h_table) cudaFreeHost(b->h_table);
+    b->d_table.release();
+    b->d_order.release();
+    b->d_queue.release();
+    b->d_slabs.release();
+  }
+  delete b;
+}
+
+int smp_b200_solve_batch(smp_ctx *ctx, smp_instance *inst, int32_t count, const smp_batch_cfg *cfg,
+                         smp_batch_stats *st) {
+  smp_batch *b = nullptr;
+  smp_batch_cfg plain = cfg ? *cfg : smp_batch_cfg{};
+  plain.use_graph = -1;  // a one-shot run gains nothing from capturing a graph
+  int rc = smp_b200_batch_create(ctx, inst, count, &plain, &b);
+  if (rc) return rc;
+  rc = smp_b200_batch_run(b, inst, st);
+  smp_b200_batch_destroy(b);
+  return rc;
+}
+
+void smp_b200_batch_instance(uint64_t seed, uint32_t b, int32_t n_lo, int32_t n_hi, int32_t *n_out,
+                             int32_t *kind_out) {
+  // Philox counter (b, 0xFFFFFFFF, tag 12, 0): word 0 draws the size, word 1
+  // the kind (the same stream the oracle restates).
+  uint32_t o[4];
+  philox4x32_10(b, 0xFFFFFFFFu, 12u, 0u, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32), o);
+  const double u = static_cast<double>(o[0]) * (1.0 / 4294967296.0);
+  const double v = static_cast<double>(n_lo) * std::exp2(u * std::log2(static_cast<double>(n_hi) / n_lo));
+  int32_t n = static_cast<int32_t>(std::floor(v));
+  n = std::min(std::max(n, n_lo), n_hi);
+  if (n_out) *n_out = n;
+  if (kind_out) *kind_out = static_cast<int32_t>(o[1] % 3u);
+}
+
+}  // extern "C"

@@ -1,0 +1,157 @@
+// batch_kernels.cuh -- many independent instances in one persistent launch.
+//
+// The reference solves one instance per engine object
+// (benchmark/smp_engine_exec.h:6-32); a batch here is a device table of
+// instances that CTAs pull from a queue, largest first.  One CTA solves one
+// instance at a time, start to finish:
+//   1. inversion: warps invert the women's rows into the CTA's own rank slab
+//      in global memory (uint16, n <= 65535), checking each row is a
+//      permutation by reading it back;
+//   2. proposals: the bid words (rank << 16 | man) and each man's position
+//      live in shared memory, and warps follow displacement chains exactly as
+//      the single-instance tail kernel does, looking ahead up to kMaxSub
+//      windows of 32 choices per step;
+//   3. match[m] = w, the proposal count and a status go back to the table.
+// The same kernel launched with one instance per launch is the plain
+// per-instance baseline the batched launch is measured against.
+#pragma once
+
+#include "common.cuh"
+#include "smp_b200.h"
+#include "step.cuh"
+
+namespace smpb200 {
+
+// Device-side row of the instance table (the host mirrors smp_instance).
+struct BatchInstance {
+  const int32_t *pref_m;
+  const int32_t *pref_w;
+  int32_t *match;
+  int32_t n;
+  int32_t status;
+  unsigned long long proposals;
+};
+
+// Shared memory for one instance of size n: bids, positions, small scalars.
+__host__ __device__ constexpr size_t batch_smem_bytes(int max_n) {
+  return static_cast<size_t>(max_n) * 4 + ((static_cast<size_t>(max_n) * 2 + 15) & ~static_cast<size_t>(15));
+}
+
+template <int kMaxSub>
+__global__ void __launch_bounds__(512) k_batch(BatchInstance *__restrict__ table, const int32_t *__restrict__ order,
+                                               int count, int *queue, uint16_t *__restrict__ slabs,
+                                               size_t slab_elems, int max_n, int dynamic) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t *sbid = reinterpret_cast<uint32_t *>(smem_raw);
+  uint16_t *spos = reinterpret_cast<uint16_t *>(smem_raw + static_cast<size_t>(max_n) * 4);
+  __shared__ int s_idx;
+  __shared__ int s_next_man;
+  __shared__ int s_status;
+  __shared__ int s_bad;
+  __shared__ unsigned long long s_props;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  uint16_t *rank = slabs + static_cast<size_t>(blockIdx.x) * slab_elems;
+
+  for (int round = 0;; ++round) {
+    if (tid == 0) s_idx = dynamic ? atomicAdd(queue, 1) : (round == 0 ? static_cast<int>(blockIdx.x) : count);
+    __syncthreads();
+    const int k = s_idx;
+    if (k >= count) return;
+    BatchInstance *inst = table + order[k];
+    const int n = inst->n;
+    const int32_t *pref_m = inst->pref_m;
+    const int32_t *pref_w = inst->pref_w;
+    if (n <= 0 || n > max_n || n > 65535) {
+      if (tid == 0) {
+        inst->status = SMP_ERR_UNSUPPORTED;
+        inst->proposals = 0;
+      }
+      __syncthreads();
+      continue;
+    }
+    for (int w = tid; w < n; w += blockDim.x) sbid[w] = 0xFFFFFFFFu;
+    if (tid == 0) {
+      s_next_man = 0;
+      s_status = 0;
+      s_bad = 0;
+      s_props = 0;
+    }
+    __syncthreads();
+
+    // 1. inversion, one row per warp, checked by reading the row back
+    bool bad = false;
+    for (int w = warp; w < n; w += nwarps) {
+      const int32_t *row = pref_w + static_cast<size_t>(w) * n;
+      uint16_t *out = rank + static_cast<size_t>(w) * n;
+      for (int r = lane; r < n; r += 32) {
+        const int m = __ldg(row + r);
+        if (static_cast<unsigned>(m) < static_cast<unsigned>(n)) {
+          out[m] = static_cast<uint16_t>(r);
+        } else {
+          bad = true;
+        }
+      }
+      __syncwarp();
+      for (int r = lane; r < n; r += 32) {
+        const int m = __ldg(row + r);
+        if (static_cast<unsigned>(m) < static_cast<unsigned>(n) && out[m] != r) bad = true;
+      }
+    }
+    if (bad) s_status = SMP_ERR_INVALID_INPUT;
+    __syncthreads();
+
+    // 2. proposal chains, warp per free man (the step the tail kernel uses)
+    {
+      const SharedBids bids{sbid, spos};
+      const auto keep_going = [&]() { return *reinterpret_cast<volatile int *>(&s_status) == 0; };
+      int m = -1, pos = 0, S = 1, bad_value = 0;
+      unsigned long long settled = 0;
+      unsigned int hops = 0;
+      while (keep_going()) {
+        if (m < 0) {
+          int i = 0;
+          if (lane == 0) i = atomicAdd(&s_next_man, 1);
+          i = __shfl_sync(kFullMask, i, 0);
+          if (i >= n) break;
+          m = i;
+          pos = 0;
+          S = 1;
+        }
+        const int rc = man_step<kMaxSub>(bids, keep_going, pref_m, rank, static_cast<const uint32_t *>(nullptr),
+                                         0, n, false, lane, m, pos, S, settled, hops, bad_value);
+        if (rc == kStepMoved || rc == kStepMatchedFree) continue;
+        if (rc == kStepBad && lane == 0) s_status = SMP_ERR_INVALID_INPUT;
+        break;
+      }
+    }
+    __syncthreads();
+
+    // 3. outputs
+    if (!s_status) {
+      unsigned long long props = 0;
+      for (int w = tid; w < n; w += blockDim.x) {
+        const uint32_t b = sbid[w];
+        if (b == 0xFFFFFFFFu) {
+          s_bad = 1;
+          continue;
+        }
+        inst->match[b & 0xFFFFu] = w;
+      }
+      for (int mm = tid; mm < n; mm += blockDim.x) props += spos[mm] + 1ull;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) props += __shfl_down_sync(kFullMask, props, off);
+      if (lane == 0) atomicAdd(&s_props, props);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      inst->status = s_status ? s_status : (s_bad ? SMP_ERR_INVALID_INPUT : SMP_OK);
+      inst->proposals = s_status || s_bad ? 0ull : s_props;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace smpb200

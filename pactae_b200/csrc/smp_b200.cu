@@ -17,6 +17,8 @@ constexpr int kDefaultPrefixK = 192;
 constexpr int kDefaultTailThreshold = 96;
 constexpr int kDefaultBulkWindow = 256;
 constexpr int kDefaultTailWindow = 256;
+constexpr int kQueryTailWindow = 32;
+constexpr int kRankTailWindow = 256;
 constexpr int kU16MaxN = 65535;
 
 inline bool valid_ctx(const smp_ctx *ctx) { return ctx != nullptr && ctx->c.stream != nullptr; }
@@ -233,7 +235,7 @@ int launch_bulk(Ctx &c, int round) {
 }
 
 template <typename RankT, int kSub>
-int launch_tail(Ctx &c, int round) {
+int launch_tail(Ctx &c, int round, int only_mode) {
   const RankT *rank = reinterpret_cast<const RankT *>(c.d_rank.ptr);
   const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
   const size_t smem = tail_smem_bytes(c.n);
@@ -242,9 +244,19 @@ int launch_tail(Ctx &c, int round) {
     return c.fail_cuda("k_tail smem attribute");
   k_tail<RankT, kSub><<<1, 1024, smem, c.stream>>>(c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(),
                                                    c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
-                                                   c.d_match.as<int32_t>(), c.n, round);
+                                                   c.d_match.as<int32_t>(), c.n, round, only_mode);
   c.launches++;
   return c.check_launch("k_tail");
+}
+
+template <typename RankT>
+int launch_tail_window(Ctx &c, int window, int round, int only_mode) {
+  switch (subs_for(window)) {
+    case 1: return launch_tail<RankT, 1>(c, round, only_mode);
+    case 2: return launch_tail<RankT, 2>(c, round, only_mode);
+    case 4: return launch_tail<RankT, 4>(c, round, only_mode);
+    default: return launch_tail<RankT, 8>(c, round, only_mode);
+  }
 }
 
 template <typename RankT>
@@ -259,12 +271,13 @@ int enqueue_round(Ctx &c, int round) {
   if (rc) return rc;
   if (round == 0 && cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
   if (c.tail_threshold <= 0) return SMP_OK;
-  switch (subs_for(c.tail_window)) {
-    case 1: return launch_tail<RankT, 1>(c, round);
-    case 2: return launch_tail<RankT, 2>(c, round);
-    case 4: return launch_tail<RankT, 4>(c, round);
-    default: return launch_tail<RankT, 8>(c, round);
-  }
+  if (round == 1 || !c.query_ok || c.tail_window_cfg > 0) return launch_tail_window<RankT>(c, c.tail_window, round, -1);
+  // Query-mode instances end in short chains (narrow look-ahead is fastest);
+  // rank-mode ones in deep scans (wide look-ahead).  Both are enqueued and the
+  // device runs the one for the mode the precheck chose.
+  rc = launch_tail_window<RankT>(c, kQueryTailWindow, round, kModeQuery);
+  if (!rc) rc = launch_tail_window<RankT>(c, kRankTailWindow, round, kModeRank);
+  return rc;
 }
 
 template <typename RankT>

@@ -30,6 +30,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "step.cuh"
 
 namespace smpb200 {
 
@@ -439,44 +440,14 @@ __global__ void __launch_bounds__(512) k_qinvert(const int32_t *__restrict__ pre
 }
 
 // ---------------------------------------------------------------------------
-// One choice of a man: his r-th woman and her rank of him.
-//   0  ok
-//   1  beyond the prefix while in query mode (rank unknown)
-//   2  out-of-range woman (reported by the caller)
-// ---------------------------------------------------------------------------
-template <typename RankT>
-__device__ __forceinline__ int load_choice(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank,
-                                           const uint32_t *__restrict__ prefix, int K, int n, bool query, int m,
-                                           int r, int &w, uint32_t &rk) {
-  if (r < K) {
-    const uint32_t e = __ldg(prefix + static_cast<size_t>(m) * K + r);
-    w = static_cast<int>(e >> 16);
-    rk = e & 0xFFFFu;
-    return e == 0xFFFFFFFFu ? 2 : 0;
-  }
-  if (query) return 1;
-  w = __ldg(pref_m + static_cast<size_t>(m) * n + r);
-  if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) return 2;
-  rk = static_cast<uint32_t>(__ldg(rank + static_cast<size_t>(w) * n + m));
-  return 0;
-}
-
-// Look-ahead: a warp examines up to kMaxSub windows of 32 choices per step
-// (a template parameter: 1, 2, 4 or 8).
-
-// ---------------------------------------------------------------------------
-// Bulk proposals.  Each warp carries one free man at a time and looks at his
-// next S*32 choices at once (S = 1 for a man just taken up, doubling up to
-// kMaxSub while whole windows reject him).  Every woman whose current partner she
-// ranks above him would reject him, so those proposals are settled by one
-// relaxed read of her bid word; for the first remaining candidate the warp
-// proposes with a 64-bit atomicMin.  If accepted and she had a partner, the
-// warp continues with the displaced man from the position stored in the
-// returned word; if she was free, the count of free women drops and the warp
-// takes a man who has not proposed yet.  Once no more than tail_threshold
-// women are free, warps hand their man to the tail queue and stop.  In query
-// mode a man whose next proposal lies beyond his prefix stops the solve for
-// the rank-mode retry round.
+// Bulk proposals on every SM.  Each warp carries one free man at a time
+// (man_step above, 64-bit bids in HBM).  A man accepted by a free woman
+// lowers the count of free women and the warp takes a man who has not
+// proposed yet; a displaced man continues in the same warp from the position
+// stored in the returned bid.  Once no more than tail_threshold women are
+// free, warps hand their man to the tail queue and stop.  In query mode a man
+// whose next proposal lies beyond his prefix stops the solve for the
+// rank-mode retry round.
 // round 0: gate Main; round 1: gate Retry (rank mode).
 // ---------------------------------------------------------------------------
 template <typename RankT, int kMaxSub>
@@ -487,7 +458,8 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
   if (!gate_open(round == 0 ? kGateMain : kGateRetry, ctrl)) return;
   const bool query = round == 0 && ld_volatile_s32(&ctrl->mode) == kModeQuery;
   const int lane = threadIdx.x & 31;
-  int m = -1, pos = 0, S = 1;
+  const GlobalBids bids{bid};
+  int m = -1, pos = 0, S = 1, bad_value = 0;
   unsigned long long settled = 0;  // proposals this warp decided (lane 0's copy is used)
   unsigned int hops = 0;           // proposals this warp saw accepted
   for (;;) {
@@ -501,92 +473,31 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
       S = 1;
     }
     int free_now = 0;
-    if (lane == 0) free_now = ld_relaxed_s32(&ctrl->free_count);
-
-    int w[kMaxSub], st[kMaxSub];
-    uint32_t rk[kMaxSub];
-    unsigned long long cur[kMaxSub];
-#pragma unroll
-    for (int s = 0; s < kMaxSub; ++s) {
-      st[s] = 3;  // past the end of the list / unused
-      cur[s] = 0;
-      rk[s] = 0xFFFFFFFFu;
-      w[s] = 0;
-      if (s < S) {
-        const int r = pos + 32 * s + lane;
-        if (r < n) {
-          st[s] = load_choice(pref_m, rank, prefix, K, n, query, m, r, w[s], rk[s]);
-          if (st[s] == 0) cur[s] = ld_relaxed_u64(bid + w[s]);
-        }
-      }
+    if (lane == 0) free_now = ld_relaxed_s32(&ctrl->free_count);  // consumed after the window loads
+    const int hold_m = m, hold_pos = pos;
+    const auto keep_going = [&]() { return __shfl_sync(kFullMask, free_now, 0) > tail_threshold; };
+    const int rc = man_step<kMaxSub>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, settled,
+                                     hops, bad_value);
+    if (rc == kStepMoved) continue;
+    if (rc == kStepMatchedFree) {
+      if (lane == 0) atomicSub(&ctrl->free_count, 1);
+      continue;
     }
-    free_now = __shfl_sync(kFullMask, free_now, 0);
-    if (free_now <= tail_threshold) {  // hand over (also how a retry stops everyone)
+    if (rc == kStepHalt) {  // hand over (also how a retry stops everyone)
       // A round-0 abort drops the men: the retry round starts from scratch.
       if (lane == 0 && !(round == 0 && ld_volatile_s32(&ctrl->retry))) {
         const int q = atomicAdd(&ctrl->tail_count, 1);
-        tail_queue[q] = make_int2(m, pos);
+        tail_queue[q] = make_int2(hold_m, hold_pos);
       }
       break;
     }
-
-    bool moved = false, stop = false;
-#pragma unroll
-    for (int s = 0; s < kMaxSub; ++s) {
-      if (s < S && !moved && !stop) {
-        const unsigned badm = __ballot_sync(kFullMask, st[s] == 2);
-        if (badm) {
-          if (lane == __ffs(badm) - 1) report(ctrl, kStatusInvalidInput, w[s]);
-          stop = true;
-        } else {
-          const unsigned beyond = __ballot_sync(kFullMask, st[s] == 1);
-          const unsigned before = beyond ? ((1u << (__ffs(beyond) - 1)) - 1u) : kFullMask;
-          unsigned cand = __ballot_sync(kFullMask, st[s] == 0 && rk[s] < bid_rank(cur[s])) & before;
-          while (cand) {
-            const int j = __ffs(cand) - 1;
-            unsigned long long old = 0;
-            if (lane == j)
-              old = atomicMin(bid + w[s], pack_bid(rk[s], static_cast<uint32_t>(m),
-                                                   static_cast<uint32_t>(pos + 32 * s + j)));
-            old = __shfl_sync(kFullMask, old, j);
-            const uint32_t rkj = __shfl_sync(kFullMask, rk[s], j);
-            if (bid_rank(old) > rkj) {  // accepted: she was free or held a worse man
-              settled += 32 * s + j + 1;
-              hops++;
-              if (old == kFree) {
-                if (lane == 0) atomicSub(&ctrl->free_count, 1);
-                m = -1;
-              } else {
-                m = static_cast<int>(bid_man(old));
-                pos = static_cast<int>(bid_pos(old)) + 1;
-                S = 1;
-              }
-              moved = true;
-              break;
-            }
-            cand &= cand - 1;  // someone better got there first
-          }
-          if (!moved && beyond) {  // query mode ran out of prefix: retry in rank mode
-            if (lane == 0) {
-              atomicExch(&ctrl->retry, 1);
-              atomicExch(&ctrl->free_count, -(1 << 30));
-            }
-            stop = true;
-          }
-        }
-      }
+    if (rc == kStepBad) {
+      if (lane == 0) report(ctrl, kStatusInvalidInput, bad_value);
+    } else if (lane == 0) {  // kStepBeyond: query mode ran out of prefix
+      atomicExch(&ctrl->retry, 1);
+      atomicExch(&ctrl->free_count, -(1 << 30));
     }
-    if (stop) break;
-    if (!moved) {
-      const int scanned = 32 * S;
-      settled += min(scanned, n - pos);
-      pos += scanned;
-      if (pos >= n) {  // rejected by every woman: the lists are not permutations
-        if (lane == 0) report(ctrl, kStatusInvalidInput, m);
-        break;
-      }
-      S = min(2 * S, kMaxSub);
-    }
+    break;
   }
   if (lane == 0 && settled) {
     atomicAdd(&ctrl->bulk_proposals, settled);
@@ -609,14 +520,15 @@ __device__ __forceinline__ void write_perfect(const int32_t *__restrict__ pref_m
 
 // ---------------------------------------------------------------------------
 // Tail.  One CTA of 32 warps.  The bid words move into shared memory as
-// rank << 16 | man (n <= 65535), and each man's position in his own list
-// into a shared 2-byte array, written before every proposal and published by
-// the acquire-release shared atomicMin.  Warps take men from the bulk
-// kernel's queue and from the men that never proposed, and follow their
-// chains as k_bulk does, with every bid read and atomic inside the SM.  At
-// the end the CTA writes match[] and the proposal count.  In query mode a man
-// beyond his prefix sets the retry flag and every warp stops.
+// rank << 16 | man (n <= 65535), and each man's position into a shared
+// 2-byte array (SharedBids).  Warps take men from the bulk kernel's queue and
+// from the men that never proposed, and follow their chains with every bid
+// read and atomic inside the SM.  At the end the CTA writes match[] and the
+// proposal count.  In query mode a man beyond his prefix sets the retry flag
+// and every warp stops.
 // round 0: gate Main (and no retry pending); round 1: gate Retry.
+// only_mode >= 0 runs the kernel only when the precheck chose that mode, so
+// the host can enqueue a narrow and a wide variant and the device keeps one.
 // ---------------------------------------------------------------------------
 template <typename RankT, int kMaxSub>
 __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pref_m,
@@ -624,7 +536,9 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
                                                   const uint32_t *__restrict__ prefix, int K,
                                                   const unsigned long long *__restrict__ bid, Control *ctrl,
                                                   const int2 *__restrict__ tail_queue,
-                                                  int32_t *__restrict__ match, int n, int round) {
+                                                  int32_t *__restrict__ match, int n, int round,
+                                                  int only_mode) {
+  if (only_mode >= 0 && round == 0 && ld_volatile_s32(&ctrl->mode) != only_mode) return;
   if (round == 0 && ld_volatile_s32(&ctrl->perfect)) {
     write_perfect(pref_m, match, n, ctrl);
     return;
@@ -662,7 +576,9 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
   }
   __syncthreads();
 
-  int m = -1, pos = 0, S = 1;
+  const SharedBids bids{sbid, spos};
+  const auto keep_going = [&]() { return *reinterpret_cast<volatile int *>(&s_abort) == 0; };
+  int m = -1, pos = 0, S = 1, bad_value = 0;
   unsigned long long settled = 0;
   unsigned int hops = 0;
   for (;;) {
@@ -681,81 +597,16 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
       }
       S = 1;
     }
-    int w[kMaxSub], st[kMaxSub];
-    uint32_t rk[kMaxSub];
-#pragma unroll
-    for (int s = 0; s < kMaxSub; ++s) {
-      st[s] = 3;
-      rk[s] = 0xFFFFFFFFu;
-      w[s] = 0;
-      if (s < S) {
-        const int r = pos + 32 * s + lane;
-        if (r < n) st[s] = load_choice(pref_m, rank, prefix, K, n, query, m, r, w[s], rk[s]);
-      }
+    const int rc = man_step<kMaxSub>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, settled,
+                                     hops, bad_value);
+    if (rc == kStepMoved || rc == kStepMatchedFree) continue;
+    if (rc == kStepBad) {
+      if (lane == 0) report(ctrl, kStatusInvalidInput, bad_value);
+    } else if (rc == kStepBeyond && lane == 0) {
+      s_abort = 1;
+      atomicExch(&ctrl->retry, 1);
     }
-    if (*reinterpret_cast<volatile int *>(&s_abort)) break;
-
-    bool moved = false, stop = false;
-#pragma unroll
-    for (int s = 0; s < kMaxSub; ++s) {
-      if (s < S && !moved && !stop) {
-        const unsigned badm = __ballot_sync(kFullMask, st[s] == 2);
-        if (badm) {
-          if (lane == __ffs(badm) - 1) report(ctrl, kStatusInvalidInput, w[s]);
-          stop = true;
-        } else {
-          const uint32_t cur = st[s] == 0 ? lds_relaxed_u32(sbid + w[s]) : 0u;
-          const unsigned beyond = __ballot_sync(kFullMask, st[s] == 1);
-          const unsigned before = beyond ? ((1u << (__ffs(beyond) - 1)) - 1u) : kFullMask;
-          unsigned cand = __ballot_sync(kFullMask, st[s] == 0 && rk[s] < (cur >> 16)) & before;
-          while (cand) {
-            const int j = __ffs(cand) - 1;
-            uint32_t old = 0;
-            int next_pos = 0;
-            if (lane == j) {
-              spos[m] = static_cast<uint16_t>(pos + 32 * s + j);
-              old = atom_min_acq_rel_shared(sbid + w[s], (rk[s] << 16) | static_cast<uint32_t>(m));
-              if ((old >> 16) > rk[s] && old != 0xFFFFFFFFu) next_pos = spos[old & 0xFFFFu] + 1;
-            }
-            old = __shfl_sync(kFullMask, old, j);
-            next_pos = __shfl_sync(kFullMask, next_pos, j);
-            const uint32_t rkj = __shfl_sync(kFullMask, rk[s], j);
-            if ((old >> 16) > rkj) {
-              settled += 32 * s + j + 1;
-              hops++;
-              if (old == 0xFFFFFFFFu) {
-                m = -1;
-              } else {
-                m = static_cast<int>(old & 0xFFFFu);
-                pos = next_pos;
-                S = 1;
-              }
-              moved = true;
-              break;
-            }
-            cand &= cand - 1;
-          }
-          if (!moved && beyond) {
-            if (lane == 0) {
-              s_abort = 1;
-              atomicExch(&ctrl->retry, 1);
-            }
-            stop = true;
-          }
-        }
-      }
-    }
-    if (stop) break;
-    if (!moved) {
-      const int scanned = 32 * S;
-      settled += min(scanned, n - pos);
-      pos += scanned;
-      if (pos >= n) {
-        if (lane == 0) report(ctrl, kStatusInvalidInput, m);
-        break;
-      }
-      S = min(2 * S, kMaxSub);
-    }
+    break;
   }
   if (lane == 0 && settled) {
     atomicAdd(&ctrl->tail_proposals, settled);

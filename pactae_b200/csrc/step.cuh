@@ -1,0 +1,230 @@
+// step.cuh -- one proposal step of a man (load a window of his choices,
+// settle rejections by reading bids, propose to the first candidate), shared
+// by the single-instance bulk and tail kernels and the batch kernel.  Only
+// inline device code and templates live here, so several translation units
+// may include it.
+#pragma once
+
+#include "common.cuh"
+
+namespace smpb200 {
+
+// ---------------------------------------------------------------------------
+// One choice of a man: his r-th woman and her rank of him.
+//   0  ok
+//   1  beyond the prefix while in query mode (rank unknown)
+//   2  out-of-range woman (reported by the caller)
+// ---------------------------------------------------------------------------
+template <typename RankT>
+__device__ __forceinline__ int load_choice(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank,
+                                           const uint32_t *__restrict__ prefix, int K, int n, bool query, int m,
+                                           int r, int &w, uint32_t &rk) {
+  if (r < K) {
+    const uint32_t e = __ldg(prefix + static_cast<size_t>(m) * K + r);
+    w = static_cast<int>(e >> 16);
+    rk = e & 0xFFFFu;
+    return e == 0xFFFFFFFFu ? 2 : 0;
+  }
+  if (query) return 1;
+  w = __ldg(pref_m + static_cast<size_t>(m) * n + r);
+  if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) return 2;
+  rk = static_cast<uint32_t>(__ldg(rank + static_cast<size_t>(w) * n + m));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// One proposal step of a man, shared by the bulk, tail and batch kernels.
+//
+// A warp looks at the man's next S windows of 32 choices (S = 1 for a man
+// just taken up, doubling up to kMaxSub while whole windows reject him).
+// Every woman whose current partner she ranks above him would reject him, so
+// those proposals are settled by one read of her bid; for the first remaining
+// candidate the warp proposes with an atomicMin.  The common case -- accepted
+// within the first window -- runs a tight single-window path; the wide path
+// (S > 1) is only entered while galloping through a deep list, and after a
+// lost race it moves on to the windows it already loaded.
+//
+// Bid storage is a policy: GlobalBids (64-bit words in HBM, the all-SM bulk
+// kernel) or SharedBids (rank << 16 | man words and 2-byte positions in
+// shared memory, one CTA).
+// ---------------------------------------------------------------------------
+constexpr int kStepMoved = 0;        // settled proposals; m / pos / S updated
+constexpr int kStepMatchedFree = 1;  // accepted by a free woman: m = -1
+constexpr int kStepBad = 2;          // invalid input (value in bad_value)
+constexpr int kStepBeyond = 3;       // query mode: next choice beyond the prefix
+constexpr int kStepHalt = 4;         // the caller's check asked to stop
+
+struct GlobalBids {
+  unsigned long long *bid;
+  __device__ __forceinline__ uint32_t cur_rank(int w) const { return bid_rank(ld_relaxed_u64(bid + w)); }
+  // Returns the replaced word if accepted, else 0 (an accepted word's rank is
+  // above the proposer's, so it is never 0).
+  __device__ __forceinline__ unsigned long long propose(int w, uint32_t rk, int m, int pos) const {
+    const unsigned long long old =
+        atomicMin(bid + w, pack_bid(rk, static_cast<uint32_t>(m), static_cast<uint32_t>(pos)));
+    return bid_rank(old) > rk ? old : 0ull;
+  }
+  // true if she was free; else the displaced man and where he resumes
+  __device__ __forceinline__ bool decode(unsigned long long res, int &m, int &pos) const {
+    if (res == kFree) return true;
+    m = static_cast<int>(bid_man(res));
+    pos = static_cast<int>(bid_pos(res)) + 1;
+    return false;
+  }
+};
+
+struct SharedBids {
+  uint32_t *sbid;  // rank << 16 | man; 0xFFFFFFFF = free
+  uint16_t *spos;  // each man's position of his current proposal
+  __device__ __forceinline__ uint32_t cur_rank(int w) const { return lds_relaxed_u32(sbid + w) >> 16; }
+  // The position is written before the release-acquire atomic publishes the
+  // man; the displaced man's position is read after it.
+  __device__ __forceinline__ unsigned long long propose(int w, uint32_t rk, int m, int pos) const {
+    spos[m] = static_cast<uint16_t>(pos);
+    const uint32_t old = atom_min_acq_rel_shared(sbid + w, (rk << 16) | static_cast<uint32_t>(m));
+    if ((old >> 16) <= rk) return 0ull;
+    const uint32_t np = old != 0xFFFFFFFFu ? spos[old & 0xFFFFu] + 1u : 0u;
+    return (static_cast<unsigned long long>(np) << 32) | old;
+  }
+  __device__ __forceinline__ bool decode(unsigned long long res, int &m, int &pos) const {
+    const uint32_t old = static_cast<uint32_t>(res);
+    if (old == 0xFFFFFFFFu) return true;
+    m = static_cast<int>(old & 0xFFFFu);
+    pos = static_cast<int>(res >> 32);
+    return false;
+  }
+};
+
+// Candidates of one window (cm), stopped by the first bad / beyond lane (em).
+// Returns kStepMoved / kStepMatchedFree with the acceptance lane in j_acc,
+// kStepBad / kStepBeyond for a stop, or -1 if the window rejected him.
+template <typename Bids>
+__device__ __forceinline__ int try_window(const Bids &bids, int lane, int w, uint32_t rk, int st, unsigned cm,
+                                          unsigned em, int m, int base, int &new_m, int &new_pos, int &j_acc,
+                                          int &bad_value) {
+  if (em) cm &= (1u << (__ffs(em) - 1)) - 1u;
+  while (cm) {
+    const int j = __ffs(cm) - 1;
+    unsigned long long res = 0ull;
+    if (lane == j) res = bids.propose(w, rk, m, base + j);
+    res = __shfl_sync(kFullMask, res, j);
+    if (res) {
+      j_acc = j;
+      return bids.decode(res, new_m, new_pos) ? kStepMatchedFree : kStepMoved;
+    }
+    cm &= cm - 1;  // someone better got there first
+  }
+  if (em) {
+    const int e = __ffs(em) - 1;
+    const int ste = __shfl_sync(kFullMask, st, e);
+    bad_value = __shfl_sync(kFullMask, w, e);
+    return ste == 2 ? kStepBad : kStepBeyond;
+  }
+  return -1;
+}
+
+template <int kMaxSub, typename RankT, typename Bids, typename Check>
+__device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, const int32_t *__restrict__ pref_m,
+                                        const RankT *__restrict__ rank, const uint32_t *__restrict__ prefix, int K,
+                                        int n, bool query, int lane, int &m, int &pos, int &S,
+                                        unsigned long long &settled, unsigned int &hops, int &bad_value) {
+  int nm = -1, np = 0, j = 0;
+  if (kMaxSub == 1 || S == 1) {
+    int w0 = 0, st0 = 3;
+    uint32_t rk0 = 0xFFFFFFFFu;
+    const int r = pos + lane;
+    if (r < n) st0 = load_choice(pref_m, rank, prefix, K, n, query, m, r, w0, rk0);
+    const uint32_t cr = st0 == 0 ? bids.cur_rank(w0) : 0u;
+    if (!keep_going()) return kStepHalt;
+    const unsigned cm = __ballot_sync(kFullMask, st0 == 0 && rk0 < cr);
+    const unsigned em = (pos + 32 > K) ? __ballot_sync(kFullMask, st0 == 1 || st0 == 2) : 0u;
+    const int rc = try_window(bids, lane, w0, rk0, st0, cm, em, m, pos, nm, np, j, bad_value);
+    if (rc == kStepMoved || rc == kStepMatchedFree) {
+      settled += j + 1;
+      hops++;
+      m = rc == kStepMatchedFree ? -1 : nm;
+      pos = np;
+      S = 1;
+      return rc;
+    }
+    if (rc >= 0) return rc;
+    settled += min(32, n - pos);
+    pos += 32;
+    if (pos >= n) {  // rejected by every woman: the lists are not permutations
+      bad_value = m;
+      return kStepBad;
+    }
+    S = min(2, kMaxSub);
+    return kStepMoved;
+  }
+  // wide path
+  int w[kMaxSub], st[kMaxSub];
+  uint32_t rk[kMaxSub], cr[kMaxSub];
+#pragma unroll
+  for (int s = 0; s < kMaxSub; ++s) {
+    st[s] = 3;
+    w[s] = 0;
+    rk[s] = 0xFFFFFFFFu;
+    cr[s] = 0u;
+    if (s < S) {
+      const int r = pos + 32 * s + lane;
+      if (r < n) {
+        st[s] = load_choice(pref_m, rank, prefix, K, n, query, m, r, w[s], rk[s]);
+        if (st[s] == 0) cr[s] = bids.cur_rank(w[s]);
+      }
+    }
+  }
+  if (!keep_going()) return kStepHalt;
+  const bool edge = pos + 32 * S > K;
+  unsigned cm[kMaxSub], em[kMaxSub];
+#pragma unroll
+  for (int s = 0; s < kMaxSub; ++s) {
+    cm[s] = 0u;
+    em[s] = 0u;
+    if (s < S) {
+      cm[s] = __ballot_sync(kFullMask, st[s] == 0 && rk[s] < cr[s]);
+      if (edge) em[s] = __ballot_sync(kFullMask, st[s] == 1 || st[s] == 2);
+    }
+  }
+  for (int s0 = 0; s0 < S;) {
+    int sstar = -1;
+#pragma unroll
+    for (int s = 0; s < kMaxSub; ++s)
+      if (sstar < 0 && s >= s0 && s < S && (cm[s] | em[s])) sstar = s;
+    if (sstar < 0) break;
+    int ws = 0, sts = 3;
+    uint32_t rks = 0xFFFFFFFFu;
+    unsigned cms = 0u, ems = 0u;
+#pragma unroll
+    for (int s = 0; s < kMaxSub; ++s) {
+      if (s == sstar) {
+        ws = w[s];
+        rks = rk[s];
+        sts = st[s];
+        cms = cm[s];
+        ems = em[s];
+      }
+    }
+    const int rc = try_window(bids, lane, ws, rks, sts, cms, ems, m, pos + 32 * sstar, nm, np, j, bad_value);
+    if (rc == kStepMoved || rc == kStepMatchedFree) {
+      settled += 32 * sstar + j + 1;
+      hops++;
+      m = rc == kStepMatchedFree ? -1 : nm;
+      pos = np;
+      S = 1;
+      return rc;
+    }
+    if (rc >= 0) return rc;
+    s0 = sstar + 1;
+  }
+  settled += min(32 * S, n - pos);
+  pos += 32 * S;
+  if (pos >= n) {
+    bad_value = m;
+    return kStepBad;
+  }
+  S = min(2 * S, kMaxSub);
+  return kStepMoved;
+}
+
+}  // namespace smpb200

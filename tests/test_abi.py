@@ -120,3 +120,12 @@ def test_oracle_generator_and_product_constants_agree():
             oracle.GEN_REF_CONGESTED, oracle.GEN_GROUPED, oracle.GEN_SOLO) == (
         pb.SMP_GEN_UNIFORM, pb.SMP_GEN_CONGESTED, pb.SMP_GEN_CORRELATED, pb.SMP_GEN_PERFECT,
         pb.SMP_GEN_REF_CONGESTED, pb.SMP_GEN_GROUPED, pb.SMP_GEN_SOLO)
+
+
+def test_batch_recipe_matches_oracle():
+    # host-only entry point: the size/kind recipe of a seeded batch mix
+    import oracle
+
+    for b in range(3000):
+        assert pb.batch_instance(5, b, 16, 4096) == oracle.batch_instance(5, b, 16, 4096)
+        assert pb.batch_instance(6, b, 64, 16384) == oracle.batch_instance(6, b, 64, 16384)
