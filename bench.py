@@ -55,6 +55,13 @@ def parse_args():
     ap.add_argument("--param", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 8192-instance batched leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
+    ap.add_argument("--batch-count", type=int, default=8192)
+    ap.add_argument("--no-plain", action="store_true", help="skip the one-launch-per-instance baseline")
+    ap.add_argument("--serving-loads", default="0.3,0.7,1.0",
+                    help="offered loads as fractions of the measured saturation (e.g. 0.1,0.2,...,1.0)")
+    ap.add_argument("--serving-requests", type=int, default=150)
     return ap.parse_args()
 
 
@@ -341,8 +348,148 @@ def run_b200(args, dist: Dist) -> dict | None:
     # CPU baseline: the reference's Mw-Par-Cpu on the same instance, rank 0, N = 1
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline and result is not None:
         result["cpu_baseline"] = cpu_baseline(args, h_pm, h_pw, match.cpu().numpy(), ctx)
+    del h_pm, h_pw
+    torch.cuda.empty_cache()
+    if not args.no_batch:
+        bres = run_batched(ctx, args, dist)
+        if result is not None:
+            result["batched"] = bres
+    torch.cuda.empty_cache()
+    if not args.no_serving:
+        sres = run_serving(ctx, args, dist)
+        if result is not None:
+            result["serving"] = sres
     ctx.close()
     return result
+
+
+KIND_PARAM = {0: 0, 1: 0, 2: 500}  # correlated: sigma = 0.05
+
+
+def run_batched(ctx, args, dist: Dist) -> dict:
+    """The batched mix: args.batch_count instances, n log-uniform in
+    [16, 4096] (seed 5), kind uniform / congested / correlated per instance,
+    inputs resident in HBM.  Batched persistent launch (CUDA graph replay)
+    against the same kernel launched once per instance."""
+    import torch
+
+    import pactae_b200 as pb
+
+    count = args.batch_count
+    metas = [pb.batch_instance(5, b, 16, 4096) for b in range(count)]
+    total = sum(n * n for n, _ in metas)
+    t0 = time.perf_counter()
+    pool_m = torch.empty(total, dtype=torch.int32, device=f"cuda:{dist.local_rank}")
+    pool_w = torch.empty(total, dtype=torch.int32, device=f"cuda:{dist.local_rank}")
+    match = torch.full((sum(n for n, _ in metas),), -1, dtype=torch.int32, device=f"cuda:{dist.local_rank}")
+    insts, off, moff = [], 0, 0
+    for b, (n, kind) in enumerate(metas):
+        pm, pw = pool_m[off:off + n * n], pool_w[off:off + n * n]
+        ctx.generate_into(kind, n, 5, pm.data_ptr(), pw.data_ptr(), salt=b, param=KIND_PARAM[kind])
+        insts.append((pm, pw, match[moff:moff + n]))
+        off += n * n
+        moff += n
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    out = {"workload": f"{count} instances, n log-uniform in [16, 4096] (seed 5), kind uniform/congested/"
+                       "correlated(sigma=0.05) per instance, inputs resident in HBM",
+           "instances": count, "entries_per_list": total, "generate_s": round(gen_s, 2)}
+    with pb.Batch(ctx, insts) as batch:
+        batch.run()  # warm-up (also the L2 is far smaller than the 97 GB of lists)
+        dist.barrier()
+        runs = []
+        for _ in range(3):
+            status, props, st = batch.run()
+            runs.append(st)
+        best = dist.max(min(r["ms"] for r in runs))  # best of 3 per rank, max over ranks
+        out.update({"batched_ms": round(best, 3), "batched_ms_runs": [round(r["ms"], 3) for r in runs],
+                    "instances_per_s": round(count * dist.world / (best * 1e-3), 1),
+                    "proposals": runs[-1]["proposals"], "failed": runs[-1]["failed"],
+                    "launches_per_run": runs[-1]["launches"]})
+        # spot parity: a sample of instances against the single-instance solve
+        for b in range(0, count, max(1, count // 16)):
+            pm, pw, mt = insts[b]
+            n = mt.numel()
+            want, _ = ctx.solve(pm.view(n, n), pw.view(n, n))
+            assert torch.equal(mt, want), f"batched instance {b} differs from its single solve"
+        if not args.no_plain:
+            _, pprops, pst = batch.run_plain()
+            assert pst["proposals"] == runs[-1]["proposals"] and pst["failed"] == 0
+            out.update({"plain_ms": round(pst["ms"], 1),
+                        "plain_instances_per_s": round(count / (pst["ms"] * 1e-3), 1),
+                        "plain_launches": pst["launches"],
+                        "batched_vs_plain": round(pst["ms"] / best, 1)})
+    del pool_m, pool_w, match, insts
+    return out
+
+
+def run_serving(ctx, args, dist: Dist) -> dict:
+    """Serving: single-instance requests, n log-uniform in [64, 16384] (seed 6),
+    the three distributions, drawn from a pool of instances resident in HBM.
+    Saturation = throughput of a burst; then Poisson arrivals at fractions of
+    it.  Latency is submission to completion (the server's clock)."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    import pactae_b200 as pb
+
+    dev = f"cuda:{dist.local_rank}"
+    pool_size = 48
+    pool = []
+    for b in range(pool_size):
+        n, kind = pb.batch_instance(6, b, 64, 16384)
+        pm, pw = ctx.generate(kind, n, seed=6, salt=b, param=KIND_PARAM[kind])
+        pool.append((pm, pw, n))
+    rng = np.random.default_rng(6)
+
+    def one_load(srv, rate, count):
+        picks = rng.integers(0, pool_size, count)
+        outs = [torch.empty(pool[i][2], dtype=torch.int32, device=dev) for i in picks]
+        gaps = rng.exponential(1.0 / rate, count) if rate else np.zeros(count)
+        tickets = [None] * count
+        results = [None] * count
+
+        def submitter():
+            t = time.perf_counter()
+            for k, i in enumerate(picks):
+                t += gaps[k]
+                delay = t - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                tickets[k] = srv.submit(pool[i][0], pool[i][1], outs[k])
+
+        th = threading.Thread(target=submitter)
+        t0 = time.perf_counter()
+        th.start()
+        for k in range(count):
+            while tickets[k] is None:
+                time.sleep(0.0002)
+            results[k] = srv.poll(tickets[k])
+        th.join()
+        wall = time.perf_counter() - t0
+        lat = np.array([r["latency_ms"] for r in results])
+        assert all(r["status"] == 0 for r in results)
+        return {"offered_per_s": round(rate, 1) if rate else None, "requests": count,
+                "solves_per_s": round(count / wall, 1), "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                "p99_ms": round(float(np.percentile(lat, 99)), 3), "mean_n": int(np.mean([pool[i][2] for i in picks]))}
+
+    with pb.Server() as srv:
+        one_load(srv, 0, 32)  # warm-up
+        sat = one_load(srv, 0, args.serving_requests)
+        saturation = sat["solves_per_s"]
+        loads = []
+        for f in [float(x) for x in args.serving_loads.split(",") if x]:
+            r = one_load(srv, f * saturation, args.serving_requests)
+            r["load"] = f
+            loads.append(r)
+        st = srv.stats()
+    return {"workload": "Poisson stream of single instances, n log-uniform in [64, 16384] (seed 6), "
+                        "uniform/congested/correlated, pool of 48 instances resident in HBM, "
+                        "64 GiB admission budget", "saturation_solves_per_s": saturation,
+            "burst": sat, "loads": loads, "waves": st["waves"], "large_path": st["large"],
+            "peak_admitted_gb": round(st["peak_bytes"] / 1e9, 2)}
 
 
 def cpu_baseline(args, h_pm, h_pw, gpu_match, ctx) -> dict:

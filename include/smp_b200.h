@@ -34,7 +34,7 @@
  *                        seeded.
  *   smp_b200_batch_*     many SmpEngineExecutor runs
  *   smp_b200_solve_batch (benchmark/smp_engine_exec.h:6-32) in one launch.
- *   smp_b200_submit / smp_b200_poll
+ *   smp_b200_server_*, smp_b200_submit / smp_b200_poll
  *                        no counterpart (serving loop on top of the solver).
  *
  * Conventions.
@@ -228,6 +228,60 @@ SMP_B200_API int smp_b200_solve_batch(smp_ctx *ctx, smp_instance *inst, int32_t 
  * Philox stream as smp_b200_generate.  Host only. */
 SMP_B200_API void smp_b200_batch_instance(uint64_t seed, uint32_t b, int32_t n_lo, int32_t n_hi, int32_t *n_out,
                                           int32_t *kind_out);
+
+/* ------------------------------------------------------------------------ */
+/* Serving: a request loop with continuous batching and HBM admission.      */
+/* ------------------------------------------------------------------------ */
+
+typedef struct smp_server smp_server;
+
+typedef struct smp_server_cfg {
+  int32_t device;          /* CUDA device ordinal                                    */
+  int32_t max_wave;        /* most requests one batched launch takes; 0 = 256        */
+  int32_t route_n;         /* requests with n above this use the all-SM pipeline;    */
+                           /* 0 = 4096                                               */
+  int32_t waves;           /* batched launches in flight at once; 0 = 2              */
+  uint64_t hbm_budget;     /* bytes of admitted requests' preference and rank        */
+                           /* matrices (10 n^2 per request); 0 = 64 GiB              */
+  int32_t block_threads;   /* threads per CTA of the batched launches; 0 = 512       */
+  int32_t ctas_per_sm;     /* CTAs per SM of a batched launch; 0 = 2                 */
+  uint64_t reserved[3];
+} smp_server_cfg;
+
+typedef struct smp_result {
+  int32_t status;          /* smp_status of the request                              */
+  int32_t n;
+  int64_t proposals;
+  double queue_ms;         /* submission to launch                                   */
+  double latency_ms;       /* submission to completion                               */
+} smp_result;
+
+typedef struct smp_server_stats {
+  int64_t submitted;
+  int64_t completed;
+  int64_t waves;           /* batched launches made                                  */
+  int64_t large;           /* requests solved by the all-SM pipeline                 */
+  int64_t admitted_bytes;  /* budget in use now                                      */
+  int64_t peak_bytes;      /* most budget ever in use                                */
+} smp_server_stats;
+
+/* Starts the serving loop (its own host thread and CUDA streams). */
+SMP_B200_API int smp_b200_server_create(const smp_server_cfg *cfg, smp_server **out);
+/* Queues one request and returns at once with its ticket.  With
+ * SMP_F_DEVICE_PTRS the lists and match_out are device pointers that must
+ * stay valid until the request completes; otherwise they are host pointers
+ * (copied in when the request is admitted, the matching copied back when it
+ * completes).  A request whose matrices alone exceed the budget is refused
+ * with SMP_ERR_BUSY. */
+SMP_B200_API int smp_b200_submit(smp_server *srv, const int32_t *pref_m, const int32_t *pref_w, int32_t n,
+                                 int32_t *match_out, uint32_t flags, int64_t *ticket);
+/* Waits up to wait_ms (negative = forever) for a request.  SMP_OK: *result
+ * holds its outcome (and the ticket is released); SMP_ERR_NOT_READY: still
+ * running; SMP_ERR_INVALID_ARG: unknown ticket. */
+SMP_B200_API int smp_b200_poll(smp_server *srv, int64_t ticket, int32_t wait_ms, smp_result *result);
+SMP_B200_API int smp_b200_server_stats(smp_server *srv, smp_server_stats *st);
+/* Finishes every submitted request, then stops the loop. */
+SMP_B200_API void smp_b200_server_destroy(smp_server *srv);
 
 /* Largest n smp_b200_solve_static accepts. */
 #define SMP_B200_STATIC_MAX_N 1024

@@ -47,10 +47,13 @@ from ._lib import (  # noqa: F401  (re-exported constants)
     smp_batch_stats,
     smp_cfg,
     smp_instance,
+    smp_result,
+    smp_server_cfg,
+    smp_server_stats,
     smp_stats,
 )
 
-__all__ = ["Batch", "Context", "SmpError", "SmpObj", "SmpEngineB200", "batch_instance", "version"]
+__all__ = ["Batch", "Server", "Context", "SmpError", "SmpObj", "SmpEngineB200", "batch_instance", "version"]
 
 
 class SmpError(RuntimeError):
@@ -323,6 +326,77 @@ class Batch:
         self._h = None
 
     def __enter__(self) -> "Batch":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The serving loop (smp_b200_server_*): submit() returns a ticket at
+    once; poll() waits for the outcome.  Requests with CUDA tensors run on
+    them in place (they must stay alive until polled); numpy requests are
+    copied in when admitted and the matching copied back."""
+
+    def __init__(self, device: int = 0, max_wave: int = 0, route_n: int = 0, waves: int = 0, hbm_budget: int = 0,
+                 block_threads: int = 0, ctas_per_sm: int = 0):
+        cfg = smp_server_cfg()
+        cfg.device = device
+        cfg.max_wave = max_wave
+        cfg.route_n = route_n
+        cfg.waves = waves
+        cfg.hbm_budget = hbm_budget
+        cfg.block_threads = block_threads
+        cfg.ctas_per_sm = ctas_per_sm
+        handle = ctypes.c_void_p()
+        _check(lib.smp_b200_server_create(ctypes.byref(cfg), ctypes.byref(handle)), "smp_b200_server_create")
+        self._h = handle
+        self._live: dict[int, tuple] = {}
+
+    def submit(self, pref_m: Any, pref_w: Any, match: Any) -> int:
+        ticket = ctypes.c_int64()
+        if _is_device_tensor(pref_m):
+            n = int(match.numel())
+            rc = lib.smp_b200_submit(self._h, ctypes.c_void_p(pref_m.data_ptr()), ctypes.c_void_p(pref_w.data_ptr()),
+                                     n, ctypes.c_void_p(match.data_ptr()), SMP_F_DEVICE_PTRS, ctypes.byref(ticket))
+            keep = (pref_m, pref_w, match)
+        else:
+            pm = _host_array(pref_m)
+            pw = _host_array(pref_w)
+            n = int(match.size)
+            rc = lib.smp_b200_submit(self._h, _ptr(pm), _ptr(pw), n, _ptr(match), 0, ctypes.byref(ticket))
+            keep = (pm, pw, match)
+        _check(rc, "smp_b200_submit")
+        self._live[ticket.value] = keep
+        return ticket.value
+
+    def poll(self, ticket: int, wait_ms: int = -1) -> dict | None:
+        res = smp_result()
+        rc = lib.smp_b200_poll(self._h, ticket, wait_ms, ctypes.byref(res))
+        if rc == SMP_ERR_NOT_READY:
+            return None
+        _check(rc, "smp_b200_poll")
+        self._live.pop(ticket, None)
+        return res.as_dict()
+
+    def stats(self) -> dict:
+        st = smp_server_stats()
+        _check(lib.smp_b200_server_stats(self._h, ctypes.byref(st)), "smp_b200_server_stats")
+        return st.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.smp_b200_server_destroy(self._h)
+        self._h = None
+        self._live.clear()
+
+    def __enter__(self) -> "Server":
         return self
 
     def __exit__(self, *exc) -> None:

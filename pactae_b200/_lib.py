@@ -62,6 +62,11 @@ ABI_SYMBOLS = (
     "smp_b200_batch_destroy",
     "smp_b200_solve_batch",
     "smp_b200_batch_instance",
+    "smp_b200_server_create",
+    "smp_b200_submit",
+    "smp_b200_poll",
+    "smp_b200_server_stats",
+    "smp_b200_server_destroy",
 )
 
 
@@ -142,6 +147,46 @@ class smp_batch_stats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class smp_server_cfg(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("max_wave", ctypes.c_int32),
+        ("route_n", ctypes.c_int32),
+        ("waves", ctypes.c_int32),
+        ("hbm_budget", ctypes.c_uint64),
+        ("block_threads", ctypes.c_int32),
+        ("ctas_per_sm", ctypes.c_int32),
+        ("reserved", ctypes.c_uint64 * 3),
+    ]
+
+
+class smp_result(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32),
+        ("n", ctypes.c_int32),
+        ("proposals", ctypes.c_int64),
+        ("queue_ms", ctypes.c_double),
+        ("latency_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class smp_server_stats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_int64),
+        ("completed", ctypes.c_int64),
+        ("waves", ctypes.c_int64),
+        ("large", ctypes.c_int64),
+        ("admitted_bytes", ctypes.c_int64),
+        ("peak_bytes", ctypes.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
 _U32 = ctypes.c_uint32
@@ -172,6 +217,11 @@ _SIGNATURES = {
     "smp_b200_solve_batch": (ctypes.c_int, [_P, ctypes.POINTER(smp_instance), _I32, ctypes.POINTER(smp_batch_cfg),
                                             ctypes.POINTER(smp_batch_stats)]),
     "smp_b200_batch_instance": (None, [_U64, _U32, _I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
+    "smp_b200_server_create": (ctypes.c_int, [ctypes.POINTER(smp_server_cfg), ctypes.POINTER(_P)]),
+    "smp_b200_submit": (ctypes.c_int, [_P, _P, _P, _I32, _P, _U32, ctypes.POINTER(ctypes.c_int64)]),
+    "smp_b200_poll": (ctypes.c_int, [_P, ctypes.c_int64, _I32, ctypes.POINTER(smp_result)]),
+    "smp_b200_server_stats": (ctypes.c_int, [_P, ctypes.POINTER(smp_server_stats)]),
+    "smp_b200_server_destroy": (None, [_P]),
 }
 
 

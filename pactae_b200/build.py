@@ -32,7 +32,7 @@ NVCC_FLAGS = [
     "-Xptxas", "-warn-spills",
 ]
 
-SOURCES = ["smp_b200.cu", "generate.cu", "batch.cu", "static_solve.cu"]
+SOURCES = ["smp_b200.cu", "generate.cu", "batch.cu", "serve.cu", "static_solve.cu"]
 
 
 def _nvcc() -> str:

@@ -106,6 +106,43 @@ void fill_batch_stats(const smp_batch &b, smp_instance *results, smp_batch_stats
 
 }  // namespace
 
+namespace smpb200 {
+
+// Used by the serving loop: launch the batch kernel on a given stream for a
+// table it owns (subs = look-ahead windows; the smem attribute is set here,
+// outside any capture).
+int launch_batch_kernel(Ctx &c, cudaStream_t s, int subs, BatchInstance *table, const int32_t *order, int count,
+                        int *queue, uint16_t *slabs, size_t slab_elems, int max_n, int grid, int block) {
+  const size_t smem = batch_smem_bytes(max_n);
+  cudaError_t e = cudaSuccess;
+  switch (subs) {
+    case 1:
+      e = cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e == cudaSuccess)
+        k_batch<1><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1);
+      break;
+    case 2:
+      e = cudaFuncSetAttribute(k_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e == cudaSuccess)
+        k_batch<2><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1);
+      break;
+    case 4:
+      e = cudaFuncSetAttribute(k_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e == cudaSuccess)
+        k_batch<4><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1);
+      break;
+    default:
+      e = cudaFuncSetAttribute(k_batch<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e == cudaSuccess)
+        k_batch<8><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1);
+      break;
+  }
+  if (e != cudaSuccess) return c.fail_cuda("k_batch smem attribute");
+  return c.check_launch("k_batch");
+}
+
+}  // namespace smpb200
+
 extern "C" {
 
 int smp_b200_batch_create(smp_ctx *ctx, const smp_instance *inst, int32_t count, const smp_batch_cfg *cfg,

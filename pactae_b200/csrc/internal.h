@@ -110,6 +110,17 @@ struct Ctx {
   }
 };
 
+// smp_b200.cu: a whole solve split into its asynchronous part and its
+// completion (the public smp_b200_solve is the two with a sync between).
+int solve_enqueue(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
+                  uint32_t flags);
+int solve_finish(Ctx &c, uint32_t flags, smp_stats *st);
+
+// batch.cu: the batch kernel on a caller's stream and table (serving loop).
+struct BatchInstance;
+int launch_batch_kernel(Ctx &c, cudaStream_t s, int subs, BatchInstance *table, const int32_t *order, int count,
+                        int *queue, uint16_t *slabs, size_t slab_elems, int max_n, int grid, int block);
+
 // generate.cu
 int generate_side(Ctx &c, int kind, int side, int n, uint64_t seed, uint32_t salt, int param,
                   int32_t *out);

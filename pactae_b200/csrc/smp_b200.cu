@@ -430,6 +430,59 @@ void fill_stats(Ctx &c, bool timed_phases) {
 
 }  // namespace
 
+namespace smpb200 {
+
+// Enqueues a whole solve on c.stream with no host round trip (stage,
+// precheck, init, core, post, the match copy, optional check, control
+// readback).  The caller synchronises the stream, then calls solve_finish.
+int solve_enqueue(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
+                  uint32_t flags) {
+  int rc = do_stage(c, pref_m, pref_w, n, flags);
+  if (rc) return rc;
+  // One stream, no host round trips: kernels read the control block.
+  rc = enqueue_precheck(c, (flags & SMP_F_NO_PRECHECK) == 0);
+  if (!rc && (flags & SMP_F_VALIDATE)) rc = enqueue_validate(c);
+  if (!rc && cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = enqueue_init(c);
+  if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = enqueue_core(c);
+  if (!rc && cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = enqueue_post(c);
+  if (!rc && (flags & SMP_F_DEVICE_PTRS)) rc = copy_match_out(c, match_out, true);
+  if (!rc && cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc && !(flags & SMP_F_DEVICE_PTRS)) rc = copy_match_out(c, match_out, false);
+  if (!rc && (flags & SMP_F_CHECK)) {
+    if (cudaEventRecord(c.ev[kEvCheckBegin], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    // The checker reuses the solve's rank matrix; only a solve that built
+    // none (perfect, or query mode) builds it here.
+    if (!rc) rc = enqueue_invert_any(c, kGateNoRank);
+    if (!rc) rc = enqueue_check(c, c.d_match.as<int32_t>());
+    if (!rc && cudaEventRecord(c.ev[kEvCheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  }
+  if (!rc) rc = read_control(c);
+  return rc;
+}
+
+// Statistics and status of a solve whose stream has completed.
+int solve_finish(Ctx &c, uint32_t flags, smp_stats *st) {
+  c.phase = 3;
+  fill_stats(c, true);
+  c.phase = 4;
+  if (flags & SMP_F_CHECK) {
+    c.stats.blocking_pairs = static_cast<int64_t>(c.h_ctrl->blocking);
+    c.stats.check_ms = elapsed(c, kEvCheckBegin, kEvCheckEnd);
+    // The checker recounts the proposals from the matching itself.
+    if (c.h_ctrl->check_proposals != c.h_ctrl->proposals && c.h_ctrl->status == 0) {
+      c.last_error = "checker proposal count differs from the solve's";
+      return SMP_ERR_CUDA;
+    }
+  }
+  if (st) *st = c.stats;
+  return control_status(c);
+}
+
+}  // namespace smpb200
+
 // ===========================================================================
 // Public ABI
 // ===========================================================================
@@ -619,45 +672,10 @@ int smp_b200_solve(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w, i
   if (!valid_ctx(ctx) || !match_out) return SMP_ERR_INVALID_ARG;
   Ctx &c = ctx->c;
   DeviceGuard g(c.device);
-  int rc = do_stage(c, pref_m, pref_w, n, flags);
-  if (rc) return rc;
-  // One stream, no host round trips: kernels read ctrl->perfect themselves.
-  rc = enqueue_precheck(c, (flags & SMP_F_NO_PRECHECK) == 0);
-  if (!rc && (flags & SMP_F_VALIDATE)) rc = enqueue_validate(c);
-  if (!rc && cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-  if (!rc) rc = enqueue_init(c);
-  if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-  if (!rc) rc = enqueue_core(c);
-  if (!rc && cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-  if (!rc) rc = enqueue_post(c);
-  if (!rc && (flags & SMP_F_DEVICE_PTRS)) rc = copy_match_out(c, match_out, true);
-  if (!rc && cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-  if (!rc && !(flags & SMP_F_DEVICE_PTRS)) rc = copy_match_out(c, match_out, false);
-  if (!rc && (flags & SMP_F_CHECK)) {
-    if (cudaEventRecord(c.ev[kEvCheckBegin], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-    // The checker reuses the solve's rank matrix; only a perfect instance
-    // (which skipped the inversion) builds it here.
-    if (!rc) rc = enqueue_invert_any(c, kGateNoRank);
-    if (!rc) rc = enqueue_check(c, c.d_match.as<int32_t>());
-    if (!rc && cudaEventRecord(c.ev[kEvCheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-  }
-  if (!rc) rc = read_control(c);
+  int rc = smpb200::solve_enqueue(c, pref_m, pref_w, n, match_out, flags);
   if (!rc) rc = c.sync("solve");
   if (rc) return rc;
-  c.phase = 3;
-  fill_stats(c, true);
-  c.phase = 4;
-  if (flags & SMP_F_CHECK) {
-    c.stats.blocking_pairs = static_cast<int64_t>(c.h_ctrl->blocking);
-    c.stats.check_ms = elapsed(c, kEvCheckBegin, kEvCheckEnd);
-    // The checker recounts the proposals from the matching itself.
-    if (c.h_ctrl->check_proposals != c.h_ctrl->proposals && c.h_ctrl->status == 0) {
-      c.last_error = "checker proposal count differs from the solve's";
-      return SMP_ERR_CUDA;
-    }
-  }
-  if (st) *st = c.stats;
-  return control_status(c);
+  return smpb200::solve_finish(c, flags, st);
 }
 
 int smp_b200_invert(smp_ctx *ctx, const int32_t *pref_w, int32_t n, int32_t *rank_out, uint32_t flags) {

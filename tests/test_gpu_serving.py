@@ -1,0 +1,77 @@
+"""The serving loop (smp_b200_server_*): requests of uneven size submitted
+in a burst are admitted against the HBM budget, batched into overlapping
+waves (and the large ones run on the all-SM pipeline concurrently), and each
+result is the same as solving that request alone.  Bit-exact."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import pactae_b200 as pb
+
+pytestmark = pytest.mark.gpu
+
+KIND_PARAM = {pb.SMP_GEN_UNIFORM: 0, pb.SMP_GEN_CONGESTED: 0, pb.SMP_GEN_CORRELATED: 500}
+
+
+def make_requests(ctx, count, seed, n_lo, n_hi):
+    import torch
+
+    reqs = []
+    for b in range(count):
+        n, kind = pb.batch_instance(seed, b, n_lo, n_hi)
+        pm, pw = ctx.generate(kind, n, seed=seed, salt=b, param=KIND_PARAM[kind])
+        reqs.append((pm, pw, torch.full((n,), -1, dtype=torch.int32, device=pm.device)))
+    return reqs
+
+
+def test_results_alone_equal_results_in_the_mix(ctx):
+    reqs = make_requests(ctx, 40, seed=6, n_lo=64, n_hi=3000)
+    alone = [ctx.solve(pm, pw) for pm, pw, _ in reqs]
+    # route_n = 1024: the larger requests take the all-SM pipeline alongside the waves
+    with pb.Server(route_n=1024, max_wave=8, waves=3) as srv:
+        tickets = [srv.submit(pm, pw, mt) for pm, pw, mt in reqs]
+        results = [srv.poll(t) for t in tickets]
+        st = srv.stats()
+    assert st["submitted"] == st["completed"] == 40
+    assert st["large"] > 0 and st["waves"] > 1
+    for (pm, pw, mt), (want, wst), res in zip(reqs, alone, results):
+        assert res["status"] == 0
+        assert np.array_equal(mt.cpu().numpy(), want.cpu().numpy())
+        assert res["proposals"] == wst["proposals"]
+        assert res["latency_ms"] >= res["queue_ms"] >= 0
+
+
+def test_host_pointer_requests(ctx):
+    reqs = make_requests(ctx, 6, seed=8, n_lo=64, n_hi=1500)
+    with pb.Server(route_n=512) as srv:
+        host = [(pm.cpu().numpy(), pw.cpu().numpy(), np.full(pm.shape[0], -1, np.int32)) for pm, pw, _ in reqs]
+        tickets = [srv.submit(*h) for h in host]
+        for t, (hpm, hpw, out) in zip(tickets, host):
+            assert srv.poll(t)["status"] == 0
+            want, _ = ctx.solve(hpm, hpw)
+            assert np.array_equal(out, want)
+
+
+def test_admission_budget_is_respected(ctx):
+    reqs = make_requests(ctx, 16, seed=12, n_lo=200, n_hi=800)
+    biggest = max(int(mt.numel()) for _, _, mt in reqs)
+    budget = 10 * biggest * biggest * 2  # room for about two requests at a time
+    with pb.Server(hbm_budget=budget, max_wave=4) as srv:
+        tickets = [srv.submit(pm, pw, mt) for pm, pw, mt in reqs]
+        assert all(srv.poll(t)["status"] == 0 for t in tickets)
+        st = srv.stats()
+    assert 0 < st["peak_bytes"] <= budget and st["admitted_bytes"] == 0
+    for pm, pw, mt in reqs:
+        want, _ = ctx.solve(pm, pw)
+        assert np.array_equal(mt.cpu().numpy(), want.cpu().numpy())
+
+
+def test_oversize_request_is_refused(ctx):
+    import torch
+
+    with pb.Server(hbm_budget=10 * 100 * 100) as srv:
+        pm, pw = ctx.generate(pb.SMP_GEN_UNIFORM, 101, seed=1)
+        with pytest.raises(pb.SmpError) as e:
+            srv.submit(pm, pw, torch.empty(101, dtype=torch.int32, device="cuda:0"))
+        assert e.value.status == pb.SMP_ERR_BUSY
