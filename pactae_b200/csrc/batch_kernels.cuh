@@ -108,6 +108,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchInstance *__restrict__ table
       const SharedBids bids{sbid, spos};
       const auto keep_going = [&]() { return *reinterpret_cast<volatile int *>(&s_status) == 0; };
       int m = -1, pos = 0, S = 1, bad_value = 0;
+      Ahead ahead;
       unsigned long long settled = 0;
       unsigned int hops = 0;
       while (keep_going()) {
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchInstance *__restrict__ table
           S = 1;
         }
         const int rc = man_step<kMaxSub>(bids, keep_going, pref_m, rank, static_cast<const uint32_t *>(nullptr),
-                                         0, n, false, lane, m, pos, S, settled, hops, bad_value);
+                                         0, n, false, lane, m, pos, S, ahead, settled, hops, bad_value);
         if (rc == kStepMoved || rc == kStepMatchedFree) continue;
         if (rc == kStepBad && lane == 0) s_status = SMP_ERR_INVALID_INPUT;
         break;

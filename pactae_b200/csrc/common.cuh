@@ -93,6 +93,15 @@ __device__ __forceinline__ int ld_volatile_s32(const int *p) {
   return *reinterpret_cast<const volatile int *>(p);
 }
 
+// Grid-strided L2 prefetch of [p, p + bytes), one request per 128-byte line.
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
+  const char *base = static_cast<const char *>(p);
+  const size_t lines = (bytes + 127) / 128;
+  const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+  for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < lines; i += stride)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(base + i * 128));
+}
+
 // Shared-memory helpers for the single-CTA tail.
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -102,12 +111,19 @@ __device__ __forceinline__ uint32_t lds_relaxed_u32(const uint32_t *p) {
   asm volatile("ld.relaxed.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(smem_addr(p)) : "memory");
   return v;
 }
-// atomicMin with acquire-release semantics at CTA scope: the release half
-// publishes the proposer's position written just before; the acquire half
-// makes the displaced man's published position visible to this thread.
-__device__ __forceinline__ uint32_t atom_min_acq_rel_shared(uint32_t *p, uint32_t v) {
+// Relaxed atomicMin on a shared word.  The proposals of the one-CTA kernels
+// use it with no fence: a release would first wait for every load the thread
+// has in flight, including the next man's window issued just before (Ahead),
+// which puts a global round trip back on the chain of displacements.  The
+// position a displaced man resumes from is read from a separate array after
+// the atomic; without ordering that read can only return one of his earlier
+// positions (only he writes it, and it only grows), and resuming there just
+// repeats proposals that are rejected again, because every woman he proposed
+// to since holds a partner she ranks above him.  The matching and the
+// proposal count (taken from the final positions) do not change.
+__device__ __forceinline__ uint32_t atom_min_relaxed_shared(uint32_t *p, uint32_t v) {
   uint32_t old;
-  asm volatile("atom.acq_rel.cta.shared::cta.min.u32 %0, [%1], %2;"
+  asm volatile("atom.relaxed.cta.shared::cta.min.u32 %0, [%1], %2;"
                : "=r"(old) : "r"(smem_addr(p)), "r"(v) : "memory");
   return old;
 }

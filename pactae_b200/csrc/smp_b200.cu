@@ -249,6 +249,17 @@ int launch_tail(Ctx &c, int round, int only_mode) {
   return c.check_launch("k_tail");
 }
 
+int launch_tail_query(Ctx &c) {
+  const size_t smem = tail_smem_bytes(c.n);
+  if (cudaFuncSetAttribute(k_tail_q, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+      cudaSuccess)
+    return c.fail_cuda("k_tail_q smem attribute");
+  k_tail_q<<<1, 1024, smem, c.stream>>>(c.pref_m, c.d_prefix.as<uint32_t>(), c.K, c.d_bid.as<unsigned long long>(),
+                                        c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(), c.d_match.as<int32_t>(), c.n);
+  c.launches++;
+  return c.check_launch("k_tail_q");
+}
+
 template <typename RankT>
 int launch_tail_window(Ctx &c, int window, int round, int only_mode) {
   switch (subs_for(window)) {
@@ -272,10 +283,10 @@ int enqueue_round(Ctx &c, int round) {
   if (round == 0 && cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
   if (c.tail_threshold <= 0) return SMP_OK;
   if (round == 1 || !c.query_ok || c.tail_window_cfg > 0) return launch_tail_window<RankT>(c, c.tail_window, round, -1);
-  // Query-mode instances end in short chains (narrow look-ahead is fastest);
-  // rank-mode ones in deep scans (wide look-ahead).  Both are enqueued and the
-  // device runs the one for the mode the precheck chose.
-  rc = launch_tail_window<RankT>(c, kQueryTailWindow, round, kModeQuery);
+  // Query-mode instances end in short chains, every choice in the prefix
+  // (k_tail_q); rank-mode ones in deep scans (wide look-ahead).  Both are
+  // enqueued and the device runs the one for the mode the precheck chose.
+  rc = launch_tail_query(c);
   if (!rc) rc = launch_tail_window<RankT>(c, kRankTailWindow, round, kModeRank);
   return rc;
 }

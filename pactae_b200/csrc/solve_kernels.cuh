@@ -458,8 +458,14 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
   if (!gate_open(round == 0 ? kGateMain : kGateRetry, ctrl)) return;
   const bool query = round == 0 && ld_volatile_s32(&ctrl->mode) == kModeQuery;
   const int lane = threadIdx.x & 31;
+  // Bring the whole prefix table into L2 (n*K*4 bytes, 23 MB at n = 30000):
+  // it was written while pref_w streamed through L2, and every later step of
+  // the solve -- this kernel and the one-SM tail -- is a chain of dependent
+  // reads of it, so each miss would cost a DRAM round trip on the chain.
+  if (prefix != nullptr) prefetch_l2(prefix, static_cast<size_t>(n) * K * sizeof(uint32_t));
   const GlobalBids bids{bid};
   int m = -1, pos = 0, S = 1, bad_value = 0;
+  Ahead ahead;
   unsigned long long settled = 0;  // proposals this warp decided (lane 0's copy is used)
   unsigned int hops = 0;           // proposals this warp saw accepted
   for (;;) {
@@ -476,7 +482,7 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
     if (lane == 0) free_now = ld_relaxed_s32(&ctrl->free_count);  // consumed after the window loads
     const int hold_m = m, hold_pos = pos;
     const auto keep_going = [&]() { return __shfl_sync(kFullMask, free_now, 0) > tail_threshold; };
-    const int rc = man_step<kMaxSub>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, settled,
+    const int rc = man_step<kMaxSub>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, ahead, settled,
                                      hops, bad_value);
     if (rc == kStepMoved) continue;
     if (rc == kStepMatchedFree) {
@@ -508,6 +514,42 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
 // Shared memory of the tail: 4-byte bid and 2-byte position per person.
 __host__ __device__ constexpr size_t tail_smem_bytes(int n) {
   return static_cast<size_t>(n) * 4 + ((static_cast<size_t>(n) * 2 + 15) & ~static_cast<size_t>(15)) + 64;
+}
+
+// The global bid words as shared ones (rank << 16 | man) plus each matched
+// man's position.  The caller synchronises.
+__device__ __forceinline__ void tail_setup(const unsigned long long *__restrict__ bid, uint32_t *sbid,
+                                           uint16_t *spos, int n) {
+  for (int w = threadIdx.x; w < n; w += blockDim.x) {
+    const unsigned long long b = bid[w];
+    if (b == kFree) {
+      sbid[w] = 0xFFFFFFFFu;
+    } else {
+      sbid[w] = (bid_rank(b) << 16) | bid_man(b);
+      spos[bid_man(b)] = static_cast<uint16_t>(bid_pos(b));
+    }
+  }
+}
+
+// match[] and the proposal count (sum of final positions + 1) from the
+// shared state, after every chain has ended.  Called by the whole CTA.
+__device__ __forceinline__ void tail_finish(const uint32_t *sbid, const uint16_t *spos, int32_t *__restrict__ match,
+                                            int n, Control *ctrl, unsigned long long *s_props) {
+  unsigned long long props = 0;
+  for (int w = threadIdx.x; w < n; w += blockDim.x) {
+    const uint32_t b = sbid[w];
+    if (b == 0xFFFFFFFFu) {
+      report(ctrl, kStatusInvalidInput, w);
+      continue;
+    }
+    match[b & 0xFFFFu] = w;
+  }
+  for (int mm = threadIdx.x; mm < n; mm += blockDim.x) props += spos[mm] + 1ull;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) props += __shfl_down_sync(kFullMask, props, off);
+  if ((threadIdx.x & 31) == 0) atomicAdd(s_props, props);
+  __syncthreads();
+  if (threadIdx.x == 0) ctrl->proposals = *s_props;
 }
 
 __device__ __forceinline__ void write_perfect(const int32_t *__restrict__ pref_m, int32_t *match, int n,
@@ -558,16 +600,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
   const int queued = ld_volatile_s32(&ctrl->tail_count);
   const int first_unstarted = min(ld_volatile_s32(&ctrl->next_man), n);
   const int total = queued + (n - first_unstarted);
-
-  for (int w = tid; w < n; w += blockDim.x) {
-    const unsigned long long b = bid[w];
-    if (b == kFree) {
-      sbid[w] = 0xFFFFFFFFu;
-    } else {
-      sbid[w] = (bid_rank(b) << 16) | bid_man(b);
-      spos[bid_man(b)] = static_cast<uint16_t>(bid_pos(b));
-    }
-  }
+  tail_setup(bid, sbid, spos, n);
   if (tid == 0) {
     s_next = 0;
     s_abort = 0;
@@ -579,6 +612,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
   const SharedBids bids{sbid, spos};
   const auto keep_going = [&]() { return *reinterpret_cast<volatile int *>(&s_abort) == 0; };
   int m = -1, pos = 0, S = 1, bad_value = 0;
+  Ahead ahead;
   unsigned long long settled = 0;
   unsigned int hops = 0;
   for (;;) {
@@ -597,7 +631,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
       }
       S = 1;
     }
-    const int rc = man_step<kMaxSub>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, settled,
+    const int rc = man_step<kMaxSub, (kMaxSub < 8)>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, ahead, settled,
                                      hops, bad_value);
     if (rc == kStepMoved || rc == kStepMatchedFree) continue;
     if (rc == kStepBad) {
@@ -614,22 +648,158 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
   }
   __syncthreads();
   if (s_abort || ld_volatile_s32(&ctrl->status)) return;
+  tail_finish(sbid, spos, match, n, ctrl, &s_props);
+}
 
-  unsigned long long props = 0;
-  for (int w = tid; w < n; w += blockDim.x) {
-    const uint32_t b = sbid[w];
-    if (b == 0xFFFFFFFFu) {
-      report(ctrl, kStatusInvalidInput, w);
+// ---------------------------------------------------------------------------
+// Query-mode tail.  The same job as k_tail for the mode uniform-like inputs
+// take, where every choice a man reaches lies in his prefix, written for the
+// shortest chain of dependent operations per displacement: the last free
+// man's chain is the critical path of the whole solve (thousands of steps,
+// one after the other, on one SM).  Per step, every lane
+//   decodes its prefix word (woman, her rank of him), reads her bid word and
+//   -- in parallel with the ballot -- the position of the man holding her;
+// one 64-bit shuffle hands the first candidate's holder, his position and
+// the proposer's rank to the warp, which issues the holder's next window at
+// once, then proposes (one relaxed shared atomic) while that load is in
+// flight.  If the atomic displaced exactly that holder the warp continues
+// with the window already loaded; otherwise (a race, rare here) it reloads.
+// The abort flag is read at the top of a step and tested at its end.  A man
+// whose next choice lies beyond his prefix stops the solve for the rank-mode
+// retry round, as in k_tail.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t prefix_word(const uint32_t *__restrict__ prefix, int K, int Kn, int m, int r) {
+  return r < Kn ? __ldg(prefix + static_cast<size_t>(m) * K + r) : 0u;
+}
+
+__global__ void __launch_bounds__(1024, 1) k_tail_q(const int32_t *__restrict__ pref_m,
+                                                    const uint32_t *__restrict__ prefix, int K,
+                                                    const unsigned long long *__restrict__ bid, Control *ctrl,
+                                                    const int2 *__restrict__ tail_queue,
+                                                    int32_t *__restrict__ match, int n) {
+  if (ld_volatile_s32(&ctrl->mode) != kModeQuery) return;
+  if (ld_volatile_s32(&ctrl->perfect)) {
+    write_perfect(pref_m, match, n, ctrl);
+    return;
+  }
+  if (!gate_open(kGateMain, ctrl)) return;
+  if (ld_volatile_s32(&ctrl->retry)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t *sbid = reinterpret_cast<uint32_t *>(smem_raw);
+  uint16_t *spos = reinterpret_cast<uint16_t *>(smem_raw + static_cast<size_t>(n) * 4);
+  __shared__ int s_next;
+  __shared__ int s_abort;
+  __shared__ unsigned long long s_props;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int Kn = min(K, n);
+
+  const int queued = ld_volatile_s32(&ctrl->tail_count);
+  const int first_unstarted = min(ld_volatile_s32(&ctrl->next_man), n);
+  const int total = queued + (n - first_unstarted);
+  tail_setup(bid, sbid, spos, n);
+  if (tid == 0) {
+    s_next = 0;
+    s_abort = 0;
+    s_props = 0;
+    ctrl->tail_men = total;
+  }
+  __syncthreads();
+
+  int m = -1, pos = 0;
+  uint32_t raw = 0;
+  unsigned long long settled = 0;
+  unsigned int hops = 0;
+  for (;;) {
+    if (m < 0) {
+      int i = 0;
+      if (lane == 0) i = atomicAdd(&s_next, 1);
+      i = __shfl_sync(kFullMask, i, 0);
+      if (i >= total) break;
+      if (i < queued) {
+        const int2 e = tail_queue[i];
+        m = e.x;
+        pos = e.y;
+      } else {
+        m = first_unstarted + (i - queued);
+        pos = 0;
+      }
+      raw = prefix_word(prefix, K, Kn, m, pos + lane);
+    }
+    const int aborted = *reinterpret_cast<volatile int *>(&s_abort);  // tested at the end of the step
+    const int r = pos + lane;
+    const bool ok = r < Kn && raw != 0xFFFFFFFFu;
+    const int w = ok ? static_cast<int>(raw >> 16) : 0;
+    const uint32_t rk = raw & 0xFFFFu;
+    const uint32_t cur = ok ? lds_relaxed_u32(sbid + w) : 0u;
+    const uint32_t hp = (ok && cur != 0xFFFFFFFFu) ? spos[cur & 0xFFFFu] : 0u;
+    unsigned cm = __ballot_sync(kFullMask, ok && rk < (cur >> 16));
+    const unsigned stop = __ballot_sync(kFullMask, r < n && !ok);
+    if (stop) cm &= (1u << (__ffs(stop) - 1)) - 1u;
+    if (cm == 0) {
+      if (stop) {  // beyond the prefix (retry in rank mode) or an invalid entry
+        if (lane == 0) {
+          const int re = pos + __ffs(stop) - 1;
+          if (re < Kn) {
+            report(ctrl, kStatusInvalidInput, m);
+          } else {
+            s_abort = 1;
+            atomicExch(&ctrl->retry, 1);
+          }
+        }
+        break;
+      }
+      settled += min(32, n - pos);
+      pos += 32;
+      if (pos >= n) {  // rejected by every woman: the lists are not permutations
+        if (lane == 0) report(ctrl, kStatusInvalidInput, m);
+        break;
+      }
+      raw = prefix_word(prefix, K, Kn, m, pos + lane);
+      if (aborted) break;
       continue;
     }
-    match[b & 0xFFFFu] = w;
+    const int j = __ffs(cm) - 1;
+    const unsigned long long info = __shfl_sync(
+        kFullMask, (static_cast<unsigned long long>(hp | (rk << 16)) << 32) | cur, j);
+    const uint32_t hw = static_cast<uint32_t>(info);
+    const int hm = static_cast<int>(hw & 0xFFFFu);
+    const int hpos = static_cast<int>((info >> 32) & 0xFFFFu) + 1;
+    const uint32_t rkj = static_cast<uint32_t>(info >> 48);
+    uint32_t next_raw = 0;
+    if (hw != 0xFFFFFFFFu) next_raw = prefix_word(prefix, K, Kn, hm, hpos + lane);
+    uint32_t old = 0;
+    if (lane == j) {
+      spos[m] = static_cast<uint16_t>(pos + j);
+      old = atom_min_relaxed_shared(sbid + w, (rk << 16) | static_cast<uint32_t>(m));
+    }
+    old = __shfl_sync(kFullMask, old, j);
+    if ((old >> 16) <= rkj) {  // someone better got there first: read the bids again
+      if (aborted) break;
+      continue;
+    }
+    settled += j + 1;
+    hops++;
+    if (old == 0xFFFFFFFFu) {
+      m = -1;
+    } else if (old == hw) {
+      m = hm;
+      pos = hpos;
+      raw = next_raw;
+    } else {
+      m = static_cast<int>(old & 0xFFFFu);
+      pos = spos[m] + 1;
+      raw = prefix_word(prefix, K, Kn, m, pos + lane);
+    }
+    if (aborted) break;
   }
-  for (int mm = tid; mm < n; mm += blockDim.x) props += spos[mm] + 1ull;
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) props += __shfl_down_sync(kFullMask, props, off);
-  if (lane == 0) atomicAdd(&s_props, props);
+  if (lane == 0 && settled) {
+    atomicAdd(&ctrl->tail_proposals, settled);
+    atomicAdd(&ctrl->tail_hops, hops);
+  }
   __syncthreads();
-  if (tid == 0) ctrl->proposals = s_props;
+  if (s_abort || ld_volatile_s32(&ctrl->status)) return;
+  tail_finish(sbid, spos, match, n, ctrl, &s_props);
 }
 
 // ---------------------------------------------------------------------------

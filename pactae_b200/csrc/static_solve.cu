@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(1024, 1) k_solve_static(const int32_t *__restr
       int next_pos = 0;
       if (lane == j) {
         spos[m] = static_cast<uint16_t>(r);
-        old = atom_min_acq_rel_shared(sbid + w, (rk << 16) | static_cast<uint32_t>(m));
+        old = atom_min_relaxed_shared(sbid + w, (rk << 16) | static_cast<uint32_t>(m));
         if ((old >> 16) > rk && old != 0xFFFFFFFFu) next_pos = spos[old & 0xFFFFu] + 1;
       }
       old = __shfl_sync(kFullMask, old, j);

@@ -10,27 +10,60 @@
 namespace smpb200 {
 
 // ---------------------------------------------------------------------------
-// One choice of a man: his r-th woman and her rank of him.
+// One choice of a man: his r-th woman and her rank of him, in two halves so
+// that the first load can be issued early (see Ahead below).
+// issue_choice: the raw word -- the packed prefix entry for r < K, else the
+// woman from pref_m (rank mode), else nothing.
+// finish_choice: decodes it (and reads the rank in rank mode).
 //   0  ok
 //   1  beyond the prefix while in query mode (rank unknown)
 //   2  out-of-range woman (reported by the caller)
+//   3  past the end of the list
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t issue_choice(const int32_t *__restrict__ pref_m,
+                                                 const uint32_t *__restrict__ prefix, int K, int n, bool query,
+                                                 int m, int r) {
+  if (r >= n) return 0u;
+  if (r < K) return __ldg(prefix + static_cast<size_t>(m) * K + r);
+  if (query) return 0u;
+  return static_cast<uint32_t>(__ldg(pref_m + static_cast<size_t>(m) * n + r));
+}
+
 template <typename RankT>
-__device__ __forceinline__ int load_choice(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank,
-                                           const uint32_t *__restrict__ prefix, int K, int n, bool query, int m,
-                                           int r, int &w, uint32_t &rk) {
+__device__ __forceinline__ int finish_choice(uint32_t raw, const RankT *__restrict__ rank, int K, int n, bool query,
+                                             int m, int r, int &w, uint32_t &rk) {
+  if (r >= n) return 3;
   if (r < K) {
-    const uint32_t e = __ldg(prefix + static_cast<size_t>(m) * K + r);
-    w = static_cast<int>(e >> 16);
-    rk = e & 0xFFFFu;
-    return e == 0xFFFFFFFFu ? 2 : 0;
+    w = static_cast<int>(raw >> 16);
+    rk = raw & 0xFFFFu;
+    return raw == 0xFFFFFFFFu ? 2 : 0;
   }
   if (query) return 1;
-  w = __ldg(pref_m + static_cast<size_t>(m) * n + r);
+  w = static_cast<int>(raw);
   if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) return 2;
   rk = static_cast<uint32_t>(__ldg(rank + static_cast<size_t>(w) * n + m));
   return 0;
 }
+
+template <typename RankT>
+__device__ __forceinline__ int load_choice(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank,
+                                           const uint32_t *__restrict__ prefix, int K, int n, bool query, int m,
+                                           int r, int &w, uint32_t &rk) {
+  return finish_choice(issue_choice(pref_m, prefix, K, n, query, m, r), rank, K, n, query, m, r, w, rk);
+}
+
+// The window of the man a warp will carry next, loaded before it is known
+// for certain.  When a warp picks its candidate, the bid word it read names
+// the man who will be displaced and (directly, or through his stored
+// position) where he resumes; his first window is issued then, so its load
+// overlaps the atomic that confirms him.  man_step uses it only when the
+// atomic displaced exactly that man at exactly that position; otherwise it is
+// ignored and the window is loaded again, so a stale guess costs time only.
+struct Ahead {
+  int m = -1;        // whose window (warp-uniform); -1: none
+  int pos = 0;       // its first position
+  uint32_t raw = 0;  // this lane's issue_choice word
+};
 
 // ---------------------------------------------------------------------------
 // One proposal step of a man, shared by the bulk, tail and batch kernels.
@@ -55,8 +88,18 @@ constexpr int kStepBeyond = 3;       // query mode: next choice beyond the prefi
 constexpr int kStepHalt = 4;         // the caller's check asked to stop
 
 struct GlobalBids {
+  using Word = unsigned long long;
   unsigned long long *bid;
+  __device__ __forceinline__ Word word(int w) const { return ld_relaxed_u64(bid + w); }
+  __device__ __forceinline__ static uint32_t rank_of(Word b) { return bid_rank(b); }
   __device__ __forceinline__ uint32_t cur_rank(int w) const { return bid_rank(ld_relaxed_u64(bid + w)); }
+  // The man a bid word holds and where he would resume; false if free.
+  __device__ __forceinline__ bool holder(Word b, int &hm, int &hp) const {
+    if (b == kFree) return false;
+    hm = static_cast<int>(bid_man(b));
+    hp = static_cast<int>(bid_pos(b)) + 1;
+    return true;
+  }
   // Returns the replaced word if accepted, else 0 (an accepted word's rank is
   // above the proposer's, so it is never 0).
   __device__ __forceinline__ unsigned long long propose(int w, uint32_t rk, int m, int pos) const {
@@ -74,14 +117,26 @@ struct GlobalBids {
 };
 
 struct SharedBids {
+  using Word = uint32_t;
   uint32_t *sbid;  // rank << 16 | man; 0xFFFFFFFF = free
   uint16_t *spos;  // each man's position of his current proposal
+  __device__ __forceinline__ Word word(int w) const { return lds_relaxed_u32(sbid + w); }
+  __device__ __forceinline__ static uint32_t rank_of(Word b) { return b >> 16; }
   __device__ __forceinline__ uint32_t cur_rank(int w) const { return lds_relaxed_u32(sbid + w) >> 16; }
-  // The position is written before the release-acquire atomic publishes the
-  // man; the displaced man's position is read after it.
+  // The position read here is a guess (no ordering with the store that
+  // published it); man_step checks it against the atomic's result.
+  __device__ __forceinline__ bool holder(Word b, int &hm, int &hp) const {
+    if (b == 0xFFFFFFFFu) return false;
+    hm = static_cast<int>(b & 0xFFFFu);
+    hp = static_cast<int>(spos[hm]) + 1;
+    return true;
+  }
+  // The position is written before the atomic publishes the man; the
+  // displaced man's position is read after it (a stale read is safe, see
+  // atom_min_relaxed_shared).
   __device__ __forceinline__ unsigned long long propose(int w, uint32_t rk, int m, int pos) const {
     spos[m] = static_cast<uint16_t>(pos);
-    const uint32_t old = atom_min_acq_rel_shared(sbid + w, (rk << 16) | static_cast<uint32_t>(m));
+    const uint32_t old = atom_min_relaxed_shared(sbid + w, (rk << 16) | static_cast<uint32_t>(m));
     if ((old >> 16) <= rk) return 0ull;
     const uint32_t np = old != 0xFFFFFFFFu ? spos[old & 0xFFFFu] + 1u : 0u;
     return (static_cast<unsigned long long>(np) << 32) | old;
@@ -123,21 +178,41 @@ __device__ __forceinline__ int try_window(const Bids &bids, int lane, int w, uin
   return -1;
 }
 
-template <int kMaxSub, typename RankT, typename Bids, typename Check>
+template <int kMaxSub, bool kAhead = true, typename RankT, typename Bids, typename Check>
 __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, const int32_t *__restrict__ pref_m,
                                         const RankT *__restrict__ rank, const uint32_t *__restrict__ prefix, int K,
-                                        int n, bool query, int lane, int &m, int &pos, int &S,
+                                        int n, bool query, int lane, int &m, int &pos, int &S, Ahead &ahead,
                                         unsigned long long &settled, unsigned int &hops, int &bad_value) {
   int nm = -1, np = 0, j = 0;
   if (kMaxSub == 1 || S == 1) {
-    int w0 = 0, st0 = 3;
+    int w0 = 0;
     uint32_t rk0 = 0xFFFFFFFFu;
     const int r = pos + lane;
-    if (r < n) st0 = load_choice(pref_m, rank, prefix, K, n, query, m, r, w0, rk0);
-    const uint32_t cr = st0 == 0 ? bids.cur_rank(w0) : 0u;
+    const uint32_t raw =
+        (kAhead && ahead.m == m && ahead.pos == pos) ? ahead.raw : issue_choice(pref_m, prefix, K, n, query, m, r);
+    if (kAhead) ahead.m = -1;
+    const int st0 = finish_choice(raw, rank, K, n, query, m, r, w0, rk0);
+    typename Bids::Word cw = 0;
+    uint32_t cr = 0u;
+    if (st0 == 0) {
+      cw = bids.word(w0);
+      cr = Bids::rank_of(cw);
+    }
     if (!keep_going()) return kStepHalt;
-    const unsigned cm = __ballot_sync(kFullMask, st0 == 0 && rk0 < cr);
+    unsigned cm = __ballot_sync(kFullMask, st0 == 0 && rk0 < cr);
     const unsigned em = (pos + 32 > K) ? __ballot_sync(kFullMask, st0 == 1 || st0 == 2) : 0u;
+    if (em) cm &= (1u << (__ffs(em) - 1)) - 1u;
+    // Issue the window of the man the first candidate would displace.
+    Ahead next;
+    if (kAhead && cm) {
+      const typename Bids::Word hw = __shfl_sync(kFullMask, cw, __ffs(cm) - 1);
+      int hm = 0, hp = 0;
+      if (bids.holder(hw, hm, hp)) {
+        next.m = hm;
+        next.pos = hp;
+        next.raw = issue_choice(pref_m, prefix, K, n, query, hm, hp + lane);
+      }
+    }
     const int rc = try_window(bids, lane, w0, rk0, st0, cm, em, m, pos, nm, np, j, bad_value);
     if (rc == kStepMoved || rc == kStepMatchedFree) {
       settled += j + 1;
@@ -145,6 +220,7 @@ __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, cons
       m = rc == kStepMatchedFree ? -1 : nm;
       pos = np;
       S = 1;
+      if (kAhead && rc == kStepMoved && next.m == nm && next.pos == np) ahead = next;
       return rc;
     }
     if (rc >= 0) return rc;
