@@ -281,40 +281,46 @@ def run_b200(args, dist: Dist) -> dict | None:
     if dist.rank == 0:
         ms_per_step = total_ms / args.steps
         peak, peak_kind = measured_peak_hbm()
-        # Algorithmic bytes per solve: 8 n^2 (inversion: read pref_w, write
-        # the rank matrix as int32) + 36 per proposal (4 B of the man's list
-        # + one 32 B sector of the rank matrix).
         P = st0["proposals"]
         b_solve = 8 * n * n + 36 * P
-        kernels = {
-            "k_invert": {"ms": st0["invert_ms"], "bytes": 8 * n * n},
-            "k_bulk": {"ms": st0["bulk_ms"], "bytes": None},
-            "k_tail": {"ms": st0["tail_ms"], "bytes": None},
-        }
-        for k in kernels.values():
-            k["gbs"] = (k["bytes"] / (k["ms"] * 1e-3) / 1e9) if k["bytes"] and k["ms"] else None
-        dominant = max(kernels, key=lambda k: kernels[k]["ms"] or 0)
-        # roofline of the inversion, the bandwidth-bound kernel
-        inv_ms = statistics.mean(s["invert_ms"] for s in steps)
-        inv_ach = 8 * n * n / (inv_ms * 1e-3) / 1e9
+        # The roofline unit is one solve: B_alg = 8 n^2 (inversion: read
+        # pref_w, write an int32 rank matrix) + 36 B per proposal (4 B of the
+        # man's list + one 32 B sector of the rank matrix), over the device
+        # time of the whole solve.
         solve_ach = b_solve / (ms_per_step * 1e-3) / 1e9
+        query = st0["mode"] == 1
+        K = 192
+        # init phase: the bytes it must move at least (query mode: pref_w once,
+        # the first K choices read twice, the bucket lists written and read,
+        # the prefix written; rank mode: pref_w read, uint16 rank written,
+        # prefix gathered)
+        init_bytes = (4 * n * n + 20 * n * K) if query else (4 * n * n + 2 * n * n + 36 * n * K)
+        init_ms = statistics.mean(s["invert_ms"] for s in steps)
+        init_ach = init_bytes / (init_ms * 1e-3) / 1e9
+        phases = {
+            "init": {"ms": round(init_ms, 4), "kernels": "k_qcount, k_qscan, k_qscatter, k_qinvert" if query
+                     else "k_invert, k_prefix", "min_bytes": init_bytes, "achieved_gbs": round(init_ach, 1),
+                     "frac": round(init_ach / peak, 4), "bound": "hbm"},
+            "bulk": {"ms": round(st0["bulk_ms"], 4), "kernels": "k_bulk", "hops": st0["bulk_hops"],
+                     "bound": "latency (dependent L2 loads and atomics)"},
+            "tail": {"ms": round(st0["tail_ms"], 4), "kernels": "k_tail_q" if query else "k_tail",
+                     "hops": st0["tail_hops"], "bound": "latency (one SM, serial displacement chains)"},
+        }
+        traffic = traffic_per_launch("solve", n)
         roofline = {
-            "kernel": "k_invert",
+            "kernel": "solve (precheck, init, k_bulk, tail; one solve = one launch unit)",
             "bound": "hbm",
-            "achieved": round(inv_ach, 1),
+            "achieved": round(solve_ach, 1),
             "peak": peak,
             "unit": "GB/s",
-            "frac": round(inv_ach / peak, 4),
+            "frac": round(solve_ach / peak, 4),
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-            "traffic": traffic_per_launch("k_invert", n),
-            "algorithmic_bytes_per_launch": 8 * n * n,
-            "launch_ms": round(inv_ms, 4),
-            "dominant_kernel_by_time": dominant,
-            "solve": {"bytes": b_solve, "ms": round(ms_per_step, 4), "achieved": round(solve_ach, 1),
-                      "frac": round(solve_ach / peak, 4),
-                      "formula": "8 n^2 + 36 P over the whole solve time"},
-            "kernels": {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in v.items()}
-                        for k, v in kernels.items()},
+            "traffic": traffic,
+            "traffic_note": "DRAM bytes per solve from ncu (profiles/), scaled from n=12000" if traffic else None,
+            "algorithmic_bytes_per_launch": b_solve,
+            "formula": "B_alg = 8 n^2 + 36 P over the solve's device time (CUDA events)",
+            "launch_ms": round(ms_per_step, 4),
+            "phases": phases,
         }
         result = {
             "metric": METRIC,
@@ -402,6 +408,13 @@ def run_batched(ctx, args, dist: Dist) -> dict:
             status, props, st = batch.run()
             runs.append(st)
         best = dist.max(min(r["ms"] for r in runs))  # best of 3 per rank, max over ranks
+        # the same roofline as a single solve, summed over the instances
+        b_alg = 8 * total + 36 * runs[-1]["proposals"]
+        peak, _ = measured_peak_hbm()
+        ach = b_alg / (best * 1e-3) / 1e9
+        out["roofline"] = {"bound": "hbm", "algorithmic_bytes": b_alg, "achieved": round(ach, 1), "peak": peak,
+                           "unit": "GB/s", "frac": round(ach / peak, 4),
+                           "formula": "sum over instances of 8 n^2 + 36 P, over the batched launch time"}
         out.update({"batched_ms": round(best, 3), "batched_ms_runs": [round(r["ms"], 3) for r in runs],
                     "instances_per_s": round(count * dist.world / (best * 1e-3), 1),
                     "proposals": runs[-1]["proposals"], "failed": runs[-1]["failed"],
