@@ -88,6 +88,11 @@ struct Ctx {
   DeviceBuf gen_keys_a, gen_keys_b, gen_seg, gen_temp, gen_aux;
   Control *h_ctrl = nullptr;  // pinned host copy of the control block
   cudaEvent_t ev[10] = {};
+  // Host-pointer solves: pref_w arrives on copy_stream in kCopyChunks row
+  // chunks, each signalled by its event (created on first use).
+  static constexpr int kCopyChunks = 16;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_chunk[kCopyChunks] = {};
   int launches = 0;  // kernels launched since the last stage / call
   smp_stats stats = {};
 

@@ -18,6 +18,8 @@ constexpr int kDefaultTailThreshold = 96;
 constexpr int kDefaultBulkWindow = 256;
 constexpr int kDefaultTailWindow = 256;
 constexpr int kQueryTailWindow = 32;
+// Host-pointer solves of at least this n stream their inputs (solve_streamed).
+constexpr int kStreamMinN = 4096;
 constexpr int kRankTailWindow = 256;
 constexpr int kU16MaxN = 65535;
 
@@ -167,8 +169,9 @@ int enqueue_prefix_gather(Ctx &c, int gate) {
 }
 
 // Query mode: bucket the (man, position) pairs of every man's first K
-// choices by woman, then answer them from each woman's row.
-int enqueue_query(Ctx &c) {
+// choices by woman (enqueue_query_index), then answer them from each
+// woman's row (enqueue_qinvert, for all rows or a chunk of them).
+int enqueue_query_index(Ctx &c) {
   const int n = c.n;
   const size_t total = static_cast<size_t>(n) * c.K;
   int rc = c.d_qcnt.ensure(sizeof(int32_t) * (static_cast<size_t>(n) + 1));
@@ -184,9 +187,11 @@ int enqueue_query(Ctx &c) {
   k_qscatter<<<grid, 256, 0, c.stream>>>(c.pref_m, n, c.K, c.d_qoff.as<int32_t>(), c.d_qcnt.as<int32_t>(),
                                          c.d_qlist.as<uint32_t>(), ctrl);
   c.launches += 3;
-  rc = c.check_launch("k_qcount/k_qscan/k_qscatter");
-  if (rc) return rc;
-  const size_t smem = row_smem_bytes<uint16_t>(n);
+  return c.check_launch("k_qcount/k_qscan/k_qscatter");
+}
+
+int enqueue_qinvert(Ctx &c, int w0, int w1) {
+  const size_t smem = row_smem_bytes<uint16_t>(c.n);
   if (cudaFuncSetAttribute(k_qinvert, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
       cudaSuccess)
     return c.fail_cuda("k_qinvert smem attribute");
@@ -195,24 +200,37 @@ int enqueue_query(Ctx &c) {
     cudaGetLastError();
     per_sm = 1;
   }
-  const int qgrid = std::min(n, c.sm_count * std::max(per_sm, 1));
-  k_qinvert<<<qgrid, 512, smem, c.stream>>>(c.pref_w, n, c.K, c.d_qoff.as<int32_t>(), c.d_qlist.as<uint32_t>(),
-                                            c.d_prefix.as<uint32_t>(), ctrl);
+  const int qgrid = std::max(1, std::min(w1 - w0, c.sm_count * std::max(per_sm, 1)));
+  k_qinvert<<<qgrid, 512, smem, c.stream>>>(c.pref_w, c.n, c.K, c.d_qoff.as<int32_t>(), c.d_qlist.as<uint32_t>(),
+                                            c.d_prefix.as<uint32_t>(), c.d_ctrl.as<Control>(), w0, w1);
   c.launches++;
   return c.check_launch("k_qinvert");
 }
 
-int enqueue_init(Ctx &c) {
+int enqueue_query(Ctx &c) {
+  const int rc = enqueue_query_index(c);
+  return rc ? rc : enqueue_qinvert(c, 0, c.n);
+}
+
+// Buffers of init and core, and every woman free (SmpEngineBamboo::InitProc
+// fills partner_rank with n, smp_engine_bamboo.cu:37).
+int init_buffers(Ctx &c) {
   const int n = c.n;
   const size_t nn = static_cast<size_t>(n) * n;
   int rc = c.d_rank.ensure(nn * c.rank_bytes);
   if (!rc) rc = c.d_bid.ensure(sizeof(unsigned long long) * n);
   if (!rc && c.K > 0) rc = c.d_prefix.ensure(sizeof(uint32_t) * static_cast<size_t>(n) * c.K);
+  if (!rc) rc = c.d_tailq.ensure(sizeof(int2) * static_cast<size_t>(n));
+  if (!rc) rc = c.d_match.ensure(sizeof(int32_t) * static_cast<size_t>(n));
   if (rc) return rc;
-  // Every woman starts free (SmpEngineBamboo::InitProc fills partner_rank
-  // with n, smp_engine_bamboo.cu:37).
   if (cudaMemsetAsync(c.d_bid.ptr, 0xFF, sizeof(unsigned long long) * n, c.stream) != cudaSuccess)
     return c.fail_cuda("bid reset");
+  return SMP_OK;
+}
+
+int enqueue_init(Ctx &c) {
+  int rc = init_buffers(c);
+  if (rc) return rc;
   if (c.query_ok) {
     rc = enqueue_query(c);
     if (rc) return rc;
@@ -291,6 +309,19 @@ int enqueue_round(Ctx &c, int round) {
   return rc;
 }
 
+// Rank-mode retry round; every kernel of it returns at once unless the
+// query mode stopped because a man went beyond his prefix.
+template <typename RankT>
+int enqueue_retry_round(Ctx &c) {
+  k_retry_reset<<<1, 1024, 0, c.stream>>>(c.d_bid.as<unsigned long long>(), c.n, c.d_ctrl.as<Control>());
+  c.launches++;
+  int rc = c.check_launch("k_retry_reset");
+  if (!rc) rc = enqueue_invert_any(c, kGateRetry);
+  if (!rc) rc = enqueue_prefix_gather(c, kGateRetry);
+  if (!rc) rc = enqueue_round<RankT>(c, 1);
+  return rc;
+}
+
 template <typename RankT>
 int enqueue_core_t(Ctx &c) {
   const int n = c.n;
@@ -300,15 +331,7 @@ int enqueue_core_t(Ctx &c) {
   c.tail_ran = c.tail_threshold > 0;
   rc = enqueue_round<RankT>(c, 0);
   if (rc || !c.query_ok) return rc;
-  // Rank-mode retry round; every kernel of it returns at once unless the
-  // query mode stopped because a man went beyond his prefix.
-  k_retry_reset<<<1, 1024, 0, c.stream>>>(c.d_bid.as<unsigned long long>(), n, c.d_ctrl.as<Control>());
-  c.launches++;
-  rc = c.check_launch("k_retry_reset");
-  if (!rc) rc = enqueue_invert_any(c, kGateRetry);
-  if (!rc) rc = enqueue_prefix_gather(c, kGateRetry);
-  if (!rc) rc = enqueue_round<RankT>(c, 1);
-  return rc;
+  return enqueue_retry_round<RankT>(c);
 }
 
 int enqueue_core(Ctx &c) { return c.rank_bytes == 2 ? enqueue_core_t<uint16_t>(c) : enqueue_core_t<int32_t>(c); }
@@ -374,12 +397,8 @@ int enqueue_check(Ctx &c, const int32_t *match) {
   return c.rank_bytes == 2 ? enqueue_check_t<uint16_t>(c, match) : enqueue_check_t<int32_t>(c, match);
 }
 
-// Bring the inputs onto the device (or adopt device pointers).
-int do_stage(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, uint32_t flags) {
-  if (!pref_m || !pref_w || n <= 0 || n > SMP_B200_MAX_N) {
-    c.last_error = "stage: null list or n out of range";
-    return SMP_ERR_INVALID_ARG;
-  }
+// Per-solve state reset and plan for size n.
+int stage_reset(Ctx &c, int32_t n) {
   c.n = n;
   c.staged = false;
   c.rank_valid = false;
@@ -389,6 +408,16 @@ int do_stage(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, ui
   c.stats.blocking_pairs = -1;
   c.launches = 0;
   plan(c);
+  return SMP_OK;
+}
+
+// Bring the inputs onto the device (or adopt device pointers).
+int do_stage(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, uint32_t flags) {
+  if (!pref_m || !pref_w || n <= 0 || n > SMP_B200_MAX_N) {
+    c.last_error = "stage: null list or n out of range";
+    return SMP_ERR_INVALID_ARG;
+  }
+  stage_reset(c, n);
   int rc = c.d_ctrl.ensure(sizeof(Control));
   if (!rc) rc = c.d_seen.ensure(((static_cast<size_t>(n) + 31) / 32) * 4);
   if (rc) return rc;
@@ -492,6 +521,110 @@ int solve_finish(Ctx &c, uint32_t flags, smp_stats *st) {
   return control_status(c);
 }
 
+// Host-pointer solve that moves only what the solve reads, overlapped with
+// the work.  A query-mode solve reads only each man's first K choices of
+// pref_m (plus his first choice for the precheck), and pref_w row by row in
+// the inversion.  So: copy the first K columns of pref_m, run the precheck
+// and read its decision; in query mode stream pref_w in row chunks on a
+// second stream and invert each chunk as it lands, and copy the rest of
+// pref_m only if a man goes beyond his prefix (the rank-mode retry).  A
+// rank-mode or perfect instance falls back to copying what it needs first.
+// Two host round trips (after the precheck and after round 0) are the price.
+bool streamed_fits(const Ctx &c, uint32_t flags) {
+  return !(flags & (SMP_F_DEVICE_PTRS | SMP_F_VALIDATE | SMP_F_CHECK)) && c.query_ok && c.K > 0 && c.K < c.n &&
+         c.tail_threshold > 0 && c.n >= kStreamMinN;
+}
+
+int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
+                   uint32_t flags, smp_stats *st) {
+  const size_t row = sizeof(int32_t) * static_cast<size_t>(n);
+  int rc = c.d_ctrl.ensure(sizeof(Control));
+  if (!rc) rc = c.d_seen.ensure(((static_cast<size_t>(n) + 31) / 32) * 4);
+  if (!rc) rc = c.d_pref_m.ensure(row * n);
+  if (!rc) rc = c.d_pref_w.ensure(row * n);
+  if (rc) return rc;
+  if (!c.copy_stream) {
+    if (cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+      return c.fail_cuda("copy stream");
+    for (auto &e : c.ev_chunk)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return c.fail_cuda("chunk event");
+  }
+  int32_t *dm = c.d_pref_m.as<int32_t>();
+  int32_t *dw = c.d_pref_w.as<int32_t>();
+  c.pref_m = dm;
+  c.pref_w = dw;
+  if (cudaEventRecord(c.ev[kEvStageBegin], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  if (cudaMemcpy2DAsync(dm, row, pref_m, row, sizeof(int32_t) * c.K, n, cudaMemcpyHostToDevice, c.stream) !=
+      cudaSuccess)
+    return c.fail_cuda("pref_m prefix copy");
+  if (cudaEventRecord(c.ev[kEvStageEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  c.staged = true;
+  rc = enqueue_precheck(c, (flags & SMP_F_NO_PRECHECK) == 0);
+  if (!rc) rc = read_control(c);
+  if (!rc) rc = c.sync("precheck");
+  if (rc) return rc;
+  c.phase = 1;
+  if (c.h_ctrl->status) return control_status(c);
+  const auto copy_rest_of_m = [&]() {
+    return cudaMemcpy2DAsync(dm + c.K, row, pref_m + c.K, row, sizeof(int32_t) * (n - c.K), n,
+                             cudaMemcpyHostToDevice, c.stream) == cudaSuccess
+               ? SMP_OK
+               : c.fail_cuda("pref_m copy");
+  };
+  const bool query = c.h_ctrl->mode == kModeQuery && !c.h_ctrl->perfect;
+  if (!query) {
+    if (!c.h_ctrl->perfect) {
+      rc = copy_rest_of_m();
+      if (!rc && cudaMemcpyAsync(dw, pref_w, row * n, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+        rc = c.fail_cuda("pref_w copy");
+    }
+    if (!rc && cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    if (!rc) rc = enqueue_init(c);
+    if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    if (!rc) rc = enqueue_core(c);
+  } else {
+    if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+    rc = init_buffers(c);
+    if (!rc) rc = enqueue_query_index(c);
+    for (int k = 0; !rc && k < Ctx::kCopyChunks; ++k) {
+      const int r0 = static_cast<int>(static_cast<int64_t>(n) * k / Ctx::kCopyChunks);
+      const int r1 = static_cast<int>(static_cast<int64_t>(n) * (k + 1) / Ctx::kCopyChunks);
+      if (r0 == r1) continue;
+      const size_t off = static_cast<size_t>(r0) * n;
+      if (cudaMemcpyAsync(dw + off, pref_w + off, row * (r1 - r0), cudaMemcpyHostToDevice, c.copy_stream) !=
+              cudaSuccess ||
+          cudaEventRecord(c.ev_chunk[k], c.copy_stream) != cudaSuccess ||
+          cudaStreamWaitEvent(c.stream, c.ev_chunk[k], 0) != cudaSuccess) {
+        rc = c.fail_cuda("pref_w chunk copy");
+        break;
+      }
+      rc = enqueue_qinvert(c, r0, r1);
+    }
+    if (!rc && cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    c.tail_ran = true;
+    if (!rc) rc = enqueue_round<uint16_t>(c, 0);
+    if (!rc) rc = read_control(c);
+    if (!rc) rc = c.sync("round 0");
+    if (!rc && c.h_ctrl->retry && !c.h_ctrl->status) {
+      rc = copy_rest_of_m();
+      if (!rc) rc = enqueue_retry_round<uint16_t>(c);
+    }
+  }
+  if (!rc && cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = enqueue_post(c);
+  if (!rc && cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = copy_match_out(c, match_out, false);
+  if (!rc) rc = read_control(c);
+  // Both streams drain before returning, even after an error: the copies
+  // read the caller's buffers.
+  const int rs = c.sync("solve");
+  if (cudaStreamSynchronize(c.copy_stream) != cudaSuccess && !rc && !rs) rc = c.fail_cuda("copy stream");
+  if (rc) return rc;
+  if (rs) return rs;
+  return solve_finish(c, flags, st);
+}
+
 }  // namespace smpb200
 
 // ===========================================================================
@@ -575,8 +708,12 @@ void smp_b200_destroy(smp_ctx *ctx) {
                          &c.d_ctrl, &c.d_match, &c.d_husband, &c.d_prank, &c.d_qcnt, &c.d_qoff, &c.d_qlist,
                          &c.gen_keys_a, &c.gen_keys_b, &c.gen_seg, &c.gen_temp, &c.gen_aux})
       b->release();
+    if (c.copy_stream) cudaStreamSynchronize(c.copy_stream);
     for (auto &e : c.ev)
       if (e) cudaEventDestroy(e);
+    for (auto &e : c.ev_chunk)
+      if (e) cudaEventDestroy(e);
+    if (c.copy_stream) cudaStreamDestroy(c.copy_stream);
     if (c.h_ctrl) cudaFreeHost(c.h_ctrl);
     if (c.stream) cudaStreamDestroy(c.stream);
   }
@@ -683,6 +820,15 @@ int smp_b200_solve(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w, i
   if (!valid_ctx(ctx) || !match_out) return SMP_ERR_INVALID_ARG;
   Ctx &c = ctx->c;
   DeviceGuard g(c.device);
+  if (!(flags & SMP_F_DEVICE_PTRS) && pref_m && pref_w && n > 0 && n <= SMP_B200_MAX_N) {
+    // The host-pointer solve moves only what it reads, overlapped with work.
+    c.n = n;
+    plan(c);
+    if (smpb200::streamed_fits(c, flags)) {
+      const int rc = stage_reset(c, n);
+      return rc ? rc : smpb200::solve_streamed(c, pref_m, pref_w, n, match_out, flags, st);
+    }
+  }
   int rc = smpb200::solve_enqueue(c, pref_m, pref_w, n, match_out, flags);
   if (!rc) rc = c.sync("solve");
   if (rc) return rc;

@@ -401,16 +401,17 @@ __global__ void k_qscatter(const int32_t *__restrict__ pref_m, int n, int K, con
   }
 }
 
+// Rows [w0, w1) (the whole matrix, or one chunk of it as it arrives).
 __global__ void __launch_bounds__(512) k_qinvert(const int32_t *__restrict__ pref_w, int n, int K,
                                                  const int32_t *__restrict__ qoff,
                                                  const uint32_t *__restrict__ qlist,
-                                                 uint32_t *__restrict__ prefix, Control *ctrl) {
+                                                 uint32_t *__restrict__ prefix, Control *ctrl, int w0, int w1) {
   if (!gate_open(kGateModeQuery, ctrl)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint16_t *srow = reinterpret_cast<uint16_t *>(smem_raw);
   const int chunks = (n + 7) / 8;
   bool bad = false;
-  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+  for (int w = w0 + static_cast<int>(blockIdx.x); w < w1; w += gridDim.x) {
     load_row(pref_w + static_cast<size_t>(w) * n, srow, srow, chunks, n, bad);
     // validation: every slot written
     const uint4 *s4 = reinterpret_cast<const uint4 *>(srow);

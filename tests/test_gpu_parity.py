@@ -106,6 +106,29 @@ def test_pipeline_variants_agree(prefix_k, tail):
             assert st["proposals"] == case["proposals"]
 
 
+# -- host-pointer solves of n >= 4096 copy only what they read -----------------
+@pytest.mark.parametrize("kind,param,prefix_k,mode", [
+    (pb.SMP_GEN_UNIFORM, 0, 0, 1),        # query mode: pref_w arrives in row chunks
+    (pb.SMP_GEN_UNIFORM, 0, 8, 2),        # men go beyond an 8-choice prefix: the rest of pref_m follows
+    (pb.SMP_GEN_CONGESTED, 0, 0, 0),      # rank mode: everything is copied first
+    (pb.SMP_GEN_CORRELATED, 500, 0, None),
+    (pb.SMP_GEN_PERFECT, 0, 0, None),     # perfect: only the first choices are read
+])
+def test_streamed_host_solve_matches_oracle(kind, param, prefix_k, mode):
+    n = 4099  # rows start off 16-byte boundaries; chunks of uneven size
+    pm, pw = oracle.generate(kind, n, 17, 0, param)
+    want, props = oracle.gs_seq(pm, pw)
+    with pb.Context(prefix_k=prefix_k) as c:
+        match, st = c.solve(pm, pw)
+        again, st2 = c.solve(pm, pw)
+    assert np.array_equal(match, want) and st["proposals"] == props
+    assert np.array_equal(again, want) and st2["proposals"] == props
+    if mode is not None:
+        assert st["mode"] == mode
+    if kind == pb.SMP_GEN_PERFECT:
+        assert st["perfect"] == 1
+
+
 def test_phase_api_and_engine_mirror(ctx):
     case = next(c for c in SMALL if c["name"] == "uniform_n2000")
     pm, pw = oracle.generate(case["kind"], case["n"], case["seed"], case["salt"], case["param"])
