@@ -405,7 +405,10 @@ def run_batched(ctx, args, dist: Dist) -> dict:
     out = {"workload": f"{count} instances, n log-uniform in [16, 4096] (seed 5), kind uniform/congested/"
                        "correlated(sigma=0.05) per instance, inputs resident in HBM",
            "instances": count, "entries_per_list": total, "generate_s": round(gen_s, 2)}
+    t_create = time.perf_counter()
     with pb.Batch(ctx, insts) as batch:
+        out["create_s"] = round(time.perf_counter() - t_create, 2)  # includes the autotuner's runs
+        out["shape"] = batch.config()
         batch.run()  # warm-up (also the L2 is far smaller than the 97 GB of lists)
         dist.barrier()
         runs = []

@@ -190,12 +190,18 @@ typedef struct smp_instance {
 #define SMP_B200_BATCH_MAX_N 16384
 
 typedef struct smp_batch_cfg {
-  int32_t block_threads;   /* threads per CTA (128..512); 0 = auto           */
-  int32_t ctas_per_sm;     /* resident CTAs per SM; 0 = auto                 */
+  int32_t block_threads;   /* threads per CTA (64..512); 0 = auto            */
+  int32_t ctas_per_sm;     /* resident CTAs per SM (1..4); 0 = auto          */
   int32_t window;          /* look-ahead choices per warp step; 0 = auto     */
   int32_t use_graph;       /* 1 (default, also 0 here) = replay a captured   */
                            /* CUDA graph; -1 = plain stream launch           */
-  int32_t reserved[4];
+  int32_t rank_smem_kb;    /* shared memory per CTA for the rank matrix of   */
+                           /* small instances (those with 2 n^2 bytes that  */
+                           /* fit stay on chip); 0 = auto, -1 = none         */
+  int32_t tune;            /* 0 = the autotuner picks every auto field on a  */
+                           /* sample of the batch (cached per device, n and  */
+                           /* batch size); -1 = fixed defaults               */
+  int32_t reserved[2];
 } smp_batch_cfg;
 
 typedef struct smp_batch_stats {
@@ -220,6 +226,10 @@ SMP_B200_API int smp_b200_batch_run(smp_batch *batch, smp_instance *results, smp
 /* The same kernel launched once per instance (the per-instance baseline). */
 SMP_B200_API int smp_b200_batch_run_plain(smp_batch *batch, smp_instance *results, smp_batch_stats *st);
 SMP_B200_API void smp_b200_batch_destroy(smp_batch *batch);
+/* The shape a batch runs with (after tuning): block_threads, ctas_per_sm,
+ * window, use_graph, rank_smem_kb (-1: none) and tune (1: chosen by the
+ * autotuner, -1: fixed). */
+SMP_B200_API int smp_b200_batch_config(const smp_batch *batch, smp_batch_cfg *out);
 /* create + run + destroy; the status and proposals of inst[] are filled in. */
 SMP_B200_API int smp_b200_solve_batch(smp_ctx *ctx, smp_instance *inst, int32_t count, const smp_batch_cfg *cfg,
                                       smp_batch_stats *st);

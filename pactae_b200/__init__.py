@@ -278,7 +278,7 @@ class Batch:
     alive while the batch is used."""
 
     def __init__(self, ctx: Context, instances, block_threads: int = 0, ctas_per_sm: int = 0, window: int = 0,
-                 use_graph: bool = True):
+                 use_graph: bool = True, rank_smem_kb: int = 0, tune: bool = True):
         self.ctx = ctx
         self._keep = list(instances)
         count = len(self._keep)
@@ -297,6 +297,8 @@ class Batch:
         cfg.ctas_per_sm = ctas_per_sm
         cfg.window = window
         cfg.use_graph = 1 if use_graph else -1
+        cfg.rank_smem_kb = rank_smem_kb
+        cfg.tune = 0 if tune else -1
         handle = ctypes.c_void_p()
         import torch
 
@@ -311,6 +313,12 @@ class Batch:
         st = smp_batch_stats()
         _check(fn(self._h, results, ctypes.byref(st)), "smp_b200_batch_run")
         return [r.status for r in results], [r.proposals for r in results], st.as_dict()
+
+    def config(self) -> dict:
+        """The shape the batch runs with (after tuning)."""
+        cfg = smp_batch_cfg()
+        _check(lib.smp_b200_batch_config(self._h, ctypes.byref(cfg)), "smp_b200_batch_config")
+        return cfg.as_dict()
 
     def run(self) -> tuple[list[int], list[int], dict]:
         """Batched persistent launch: (statuses, proposals, stats)."""

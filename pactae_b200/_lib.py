@@ -59,7 +59,7 @@ ABI_SYMBOLS = (
     "smp_b200_batch_create",
     "smp_b200_batch_run",
     "smp_b200_batch_run_plain",
-    "smp_b200_batch_destroy",
+    "smp_b200_batch_destroy", "smp_b200_batch_config",
     "smp_b200_solve_batch",
     "smp_b200_batch_instance",
     "smp_b200_server_create",
@@ -130,8 +130,13 @@ class smp_batch_cfg(ctypes.Structure):
         ("ctas_per_sm", ctypes.c_int32),
         ("window", ctypes.c_int32),
         ("use_graph", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("rank_smem_kb", ctypes.c_int32),
+        ("tune", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 2),
     ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
 class smp_batch_stats(ctypes.Structure):
@@ -214,6 +219,7 @@ _SIGNATURES = {
     "smp_b200_batch_run": (ctypes.c_int, [_P, ctypes.POINTER(smp_instance), ctypes.POINTER(smp_batch_stats)]),
     "smp_b200_batch_run_plain": (ctypes.c_int, [_P, ctypes.POINTER(smp_instance), ctypes.POINTER(smp_batch_stats)]),
     "smp_b200_batch_destroy": (None, [_P]),
+    "smp_b200_batch_config": (ctypes.c_int, [_P, ctypes.POINTER(smp_batch_cfg)]),
     "smp_b200_solve_batch": (ctypes.c_int, [_P, ctypes.POINTER(smp_instance), _I32, ctypes.POINTER(smp_batch_cfg),
                                             ctypes.POINTER(smp_batch_stats)]),
     "smp_b200_batch_instance": (None, [_U64, _U32, _I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),

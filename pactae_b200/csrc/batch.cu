@@ -3,7 +3,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <numeric>
+#include <tuple>
 #include <vector>
 
 #include "batch_kernels.cuh"
@@ -23,6 +26,10 @@ struct smp_batch {
   int block = 512;
   int grid = 0;
   int subs = 8;
+  int per_sm = 2;
+  int rank_kb = 64;        // shared rank region per CTA (KB)
+  int rank_smem_elems = 0;
+  bool tuned = false;      // the autotuner chose the shape
   bool use_graph = true;
   size_t slab_elems = 0;
   size_t smem = 0;
@@ -47,9 +54,10 @@ int subs_for_window(int window) {
 }
 
 template <int kSub>
-int launch_batch_t(smp_batch &b, cudaStream_t s, int grid, const int32_t *order, int count, int dynamic) {
-  k_batch<kSub><<<grid, b.block, b.smem, s>>>(b.d_table.as<BatchInstance>(), order, count, b.d_queue.as<int>(),
-                                              b.d_slabs.as<uint16_t>(), b.slab_elems, b.max_n, dynamic);
+int launch_batch_t(smp_batch &b, cudaStream_t s, int grid, const int32_t *order, int count, int dynamic,
+                   BatchInstance *table) {
+  k_batch<kSub><<<grid, b.block, b.smem, s>>>(table, order, count, b.d_queue.as<int>(), b.d_slabs.as<uint16_t>(),
+                                              b.slab_elems, b.max_n, dynamic, b.rank_smem_elems);
   return b.ctx->c.check_launch("k_batch");
 }
 
@@ -65,13 +73,107 @@ int set_batch_attribute(smp_batch &b) {
   return e == cudaSuccess ? SMP_OK : b.ctx->c.fail_cuda("k_batch smem attribute");
 }
 
-int launch_batch(smp_batch &b, cudaStream_t s, int grid, const int32_t *order, int count, int dynamic) {
+int launch_batch(smp_batch &b, cudaStream_t s, int grid, const int32_t *order, int count, int dynamic,
+                 BatchInstance *table = nullptr) {
+  if (!table) table = b.d_table.as<BatchInstance>();
   switch (b.subs) {
-    case 1: return launch_batch_t<1>(b, s, grid, order, count, dynamic);
-    case 2: return launch_batch_t<2>(b, s, grid, order, count, dynamic);
-    case 4: return launch_batch_t<4>(b, s, grid, order, count, dynamic);
-    default: return launch_batch_t<8>(b, s, grid, order, count, dynamic);
+    case 1: return launch_batch_t<1>(b, s, grid, order, count, dynamic, table);
+    case 2: return launch_batch_t<2>(b, s, grid, order, count, dynamic, table);
+    case 4: return launch_batch_t<4>(b, s, grid, order, count, dynamic, table);
+    default: return launch_batch_t<8>(b, s, grid, order, count, dynamic, table);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Shapes and the autotuner.  A shape is the CTA size, CTAs per SM, the
+// look-ahead window and the shared rank region (the size threshold below
+// which an instance's rank matrix stays on chip: n*n*2 bytes must fit).  The
+// kernel is compiled for at most 64 registers (two 512-thread CTAs per SM),
+// so block * ctas_per_sm <= 1024.
+// ---------------------------------------------------------------------------
+struct Shape {
+  int block, per_sm, subs, rank_kb;
+};
+
+size_t shape_smem(int max_n, int rank_kb) {
+  return batch_smem_bytes(max_n) + static_cast<size_t>(std::max(rank_kb, 0)) * 1024;
+}
+
+bool shape_fits(const Ctx &c, int max_n, const Shape &sh) {
+  const size_t smem = shape_smem(max_n, sh.rank_kb);
+  int per_sm_bytes = 0;
+  cudaDeviceGetAttribute(&per_sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c.device);
+  return smem <= c.smem_optin && static_cast<size_t>(sh.per_sm) * (smem + 1024) <= static_cast<size_t>(per_sm_bytes) &&
+         sh.block * sh.per_sm <= 1024 && sh.block >= 64 && sh.block <= 512;
+}
+
+int apply_shape(smp_batch &b, const Shape &sh) {
+  const Ctx &c = b.ctx->c;
+  b.block = sh.block;
+  b.per_sm = sh.per_sm;
+  b.subs = sh.subs;
+  b.rank_kb = sh.rank_kb;
+  b.rank_smem_elems = sh.rank_kb > 0 ? sh.rank_kb * 512 : 0;
+  b.smem = shape_smem(b.max_n, sh.rank_kb);
+  const size_t slab_bytes = b.slab_elems * sizeof(uint16_t);
+  const int by_budget = static_cast<int>(std::max<size_t>(1, kSlabBudget / slab_bytes));
+  b.grid = std::max(1, std::min({c.sm_count * std::min(sh.per_sm, 4), by_budget, b.count}));
+  return set_batch_attribute(b);
+}
+
+// Tuned shapes, per device, largest n and batch size (powers of two).
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, Shape> g_tuned;
+
+// Runs the kernel over the sample table and returns its device time.
+float time_shape(smp_batch &b, const Shape &sh, BatchInstance *sample, const int32_t *order, int k) {
+  if (apply_shape(b, sh)) return 1e30f;
+  Ctx &c = b.ctx->c;
+  float best = 1e30f;
+  for (int rep = 0; rep < 1; ++rep) {
+    if (cudaMemsetAsync(b.d_queue.ptr, 0, sizeof(int), c.stream) != cudaSuccess ||
+        cudaEventRecord(b.ev0, c.stream) != cudaSuccess ||
+        launch_batch(b, c.stream, std::min(b.grid, k), order, k, 1, sample) != SMP_OK ||
+        cudaEventRecord(b.ev1, c.stream) != cudaSuccess || cudaStreamSynchronize(c.stream) != cudaSuccess) {
+      cudaGetLastError();
+      return 1e30f;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b.ev0, b.ev1);
+    best = std::min(best, ms);
+  }
+  return best;
+}
+
+// Coordinate descent over the shapes, timed on the batch itself (a sample
+// would not do: the largest instances sit on single CTAs, and a sample's
+// time is their span rather than the batch's throughput): window, then CTA
+// size and count, then the shared rank region.  Fields the caller fixed are
+// not searched.  Each candidate costs one batched run.
+Shape autotune(smp_batch &b, Shape start, const smp_batch_cfg *cfg) {
+  Ctx &c = b.ctx->c;
+  BatchInstance *sample = b.d_table.as<BatchInstance>();
+  const int32_t *order = b.d_order.as<int32_t>();
+  const int k = b.count;
+  Shape best = start;
+  time_shape(b, best, sample, order, k);  // warm-up
+  float best_t = time_shape(b, best, sample, order, k);
+  const auto consider = [&](Shape sh) {
+    if (!shape_fits(c, b.max_n, sh)) return;
+    const float ms = time_shape(b, sh, sample, order, k);
+    if (ms < best_t) {
+      best_t = ms;
+      best = sh;
+    }
+  };
+  if (!(cfg && cfg->window > 0))
+    for (int subs : {1, 2, 4, 8}) consider({best.block, best.per_sm, subs, best.rank_kb});
+  if (!(cfg && (cfg->block_threads > 0 || cfg->ctas_per_sm > 0)))
+    for (auto bp : {std::pair<int, int>{512, 1}, {512, 2}, {256, 2}, {256, 4}})
+      consider({bp.first, bp.second, best.subs, best.rank_kb});
+  if (!(cfg && cfg->rank_smem_kb != 0))
+    for (int kb : {0, 32, 64}) consider({best.block, best.per_sm, best.subs, kb});
+  return best;
 }
 
 // The batched step: reset the queue, run the persistent kernel, copy the
@@ -112,29 +214,30 @@ namespace smpb200 {
 // table it owns (subs = look-ahead windows; the smem attribute is set here,
 // outside any capture).
 int launch_batch_kernel(Ctx &c, cudaStream_t s, int subs, BatchInstance *table, const int32_t *order, int count,
-                        int *queue, uint16_t *slabs, size_t slab_elems, int max_n, int grid, int block) {
-  const size_t smem = batch_smem_bytes(max_n);
+                        int *queue, uint16_t *slabs, size_t slab_elems, int max_n, int grid, int block,
+                        int rank_smem_elems) {
+  const size_t smem = batch_smem_bytes(max_n) + static_cast<size_t>(rank_smem_elems) * 2;
   cudaError_t e = cudaSuccess;
   switch (subs) {
     case 1:
       e = cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
       if (e == cudaSuccess)
-        k_batch<1><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1);
+        k_batch<1><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1, rank_smem_elems);
       break;
     case 2:
       e = cudaFuncSetAttribute(k_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
       if (e == cudaSuccess)
-        k_batch<2><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1);
+        k_batch<2><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1, rank_smem_elems);
       break;
     case 4:
       e = cudaFuncSetAttribute(k_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
       if (e == cudaSuccess)
-        k_batch<4><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1);
+        k_batch<4><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1, rank_smem_elems);
       break;
     default:
       e = cudaFuncSetAttribute(k_batch<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
       if (e == cudaSuccess)
-        k_batch<8><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1);
+        k_batch<8><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1, rank_smem_elems);
       break;
   }
   if (e != cudaSuccess) return c.fail_cuda("k_batch smem attribute");
@@ -168,30 +271,40 @@ int smp_b200_batch_create(smp_ctx *ctx, const smp_instance *inst, int32_t count,
   std::iota(b->order.begin(), b->order.end(), 0);
   std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return inst[x].n > inst[y].n; });
 
-  b->block = (cfg && cfg->block_threads > 0) ? std::min(512, std::max(64, cfg->block_threads / 32 * 32)) : 512;
-  b->subs = subs_for_window(cfg ? cfg->window : 0);
+  // Shape: fixed fields from cfg, the rest tuned (or defaults with tune = -1).
+  Shape sh{512, 2, 1, 32};  // the best shape on the 8192-instance mix
+  if (cfg && cfg->block_threads > 0) sh.block = std::min(512, std::max(64, cfg->block_threads / 32 * 32));
+  if (cfg && cfg->ctas_per_sm > 0) sh.per_sm = std::min(4, cfg->ctas_per_sm);
+  else if (cfg && cfg->block_threads > 0) sh.per_sm = std::max(1, 1024 / sh.block);
+  if (cfg && cfg->window > 0) sh.subs = subs_for_window(cfg->window);
+  if (cfg && cfg->rank_smem_kb != 0) sh.rank_kb = std::max(0, cfg->rank_smem_kb);
   b->use_graph = !(cfg && cfg->use_graph < 0);
-  b->smem = batch_smem_bytes(b->max_n);
-  if (b->smem > c.smem_optin) {
+  const bool want_tune = !(cfg && cfg->tune < 0) &&
+                         !(cfg && cfg->block_threads > 0 && cfg->ctas_per_sm > 0 && cfg->window > 0 &&
+                           cfg->rank_smem_kb != 0);
+  // Without tuning, shrink a default shape that does not fit (large max_n).
+  while (!shape_fits(c, b->max_n, sh) && sh.rank_kb > 0) sh.rank_kb -= 32;
+  if (!shape_fits(c, b->max_n, sh) && !(cfg && cfg->ctas_per_sm > 0)) sh.per_sm = 1;
+  if (shape_smem(b->max_n, sh.rank_kb) > c.smem_optin) {
     delete b;
     return SMP_ERR_UNSUPPORTED;
-  }
-  int per_sm = (cfg && cfg->ctas_per_sm > 0) ? cfg->ctas_per_sm : 0;
-  if (per_sm == 0) {
-    // as many as fit (shared memory and threads), at most 4
-    const int by_threads = 2048 / b->block;
-    const int by_smem = static_cast<int>(std::max<size_t>(1, (c.smem_optin + 1024) / (b->smem + 1024)));
-    per_sm = std::max(1, std::min(4, std::min(by_threads, by_smem)));
   }
   b->slab_elems = static_cast<size_t>(b->max_n) * b->max_n;
   const size_t slab_bytes = b->slab_elems * sizeof(uint16_t);
   const int by_budget = static_cast<int>(std::max<size_t>(1, kSlabBudget / slab_bytes));
-  b->grid = std::max(1, std::min({c.sm_count * per_sm, by_budget, count}));
+  const int max_grid = std::max(1, std::min({c.sm_count * 4, by_budget, count}));  // any tuned shape fits
+  b->block = sh.block;
+  b->per_sm = sh.per_sm;
+  b->subs = sh.subs;
+  b->rank_kb = sh.rank_kb;
+  b->rank_smem_elems = sh.rank_kb * 512;
+  b->smem = shape_smem(b->max_n, sh.rank_kb);
+  b->grid = std::max(1, std::min({c.sm_count * sh.per_sm, by_budget, count}));
 
   int rc = b->d_table.ensure(sizeof(BatchInstance) * count);
   if (!rc) rc = b->d_order.ensure(sizeof(int32_t) * count);
   if (!rc) rc = b->d_queue.ensure(sizeof(int));
-  if (!rc) rc = b->d_slabs.ensure(slab_bytes * b->grid);
+  if (!rc) rc = b->d_slabs.ensure(slab_bytes * max_grid);
   if (!rc && cudaMallocHost(reinterpret_cast<void **>(&b->h_table), sizeof(smp_instance) * count) != cudaSuccess) {
     cudaGetLastError();
     rc = SMP_ERR_OOM;
@@ -215,7 +328,25 @@ int smp_b200_batch_create(smp_ctx *ctx, const smp_instance *inst, int32_t count,
     smp_b200_batch_destroy(b);
     return SMP_ERR_CUDA;
   }
-  rc = set_batch_attribute(*b);
+  if (want_tune) {
+    const auto key = std::make_tuple(c.device, b->max_n, 31 - __builtin_clz(static_cast<unsigned>(count)));
+    bool cached = false;
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      auto it = g_tuned.find(key);
+      if (it != g_tuned.end()) {
+        sh = it->second;
+        cached = true;
+      }
+    }
+    if (!cached) {
+      sh = autotune(*b, sh, cfg);
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      g_tuned[key] = sh;
+    }
+    b->tuned = true;
+  }
+  rc = apply_shape(*b, sh);
   if (rc) {
     smp_b200_batch_destroy(b);
     return rc;
@@ -282,6 +413,18 @@ int smp_b200_batch_run_plain(smp_batch *b, smp_instance *results, smp_batch_stat
   float ms = 0.f;
   cudaEventElapsedTime(&ms, b->ev0, b->ev1);
   fill_batch_stats(*b, results, st, ms, b->count);
+  return SMP_OK;
+}
+
+int smp_b200_batch_config(const smp_batch *b, smp_batch_cfg *out) {
+  if (!b || !out) return SMP_ERR_INVALID_ARG;
+  *out = smp_batch_cfg{};
+  out->block_threads = b->block;
+  out->ctas_per_sm = b->per_sm;
+  out->window = 32 * b->subs;
+  out->use_graph = b->exec ? 1 : -1;
+  out->rank_smem_kb = b->rank_kb > 0 ? b->rank_kb : -1;
+  out->tune = b->tuned ? 1 : -1;
   return SMP_OK;
 }
 

@@ -4,9 +4,10 @@
 // (benchmark/smp_engine_exec.h:6-32); a batch here is a device table of
 // instances that CTAs pull from a queue, largest first.  One CTA solves one
 // instance at a time, start to finish:
-//   1. inversion: warps invert the women's rows into the CTA's own rank slab
-//      in global memory (uint16, n <= 65535), checking each row is a
-//      permutation by reading it back;
+//   1. inversion: warps invert the women's rows into a uint16 rank matrix --
+//      in shared memory when it fits the CTA's rank region (small
+//      instances), else in the CTA's own slab in global memory -- checking
+//      each row is a permutation by reading it back;
 //   2. proposals: the bid words (rank << 16 | man) and each man's position
 //      live in shared memory, and warps follow displacement chains exactly as
 //      the single-instance tail kernel does, looking ahead up to kMaxSub
@@ -32,18 +33,23 @@ struct BatchInstance {
   unsigned long long proposals;
 };
 
-// Shared memory for one instance of size n: bids, positions, small scalars.
+// Shared memory for one instance of size n: bids and positions, padded to
+// 16 bytes; the rank region for small instances follows.
 __host__ __device__ constexpr size_t batch_smem_bytes(int max_n) {
-  return static_cast<size_t>(max_n) * 4 + ((static_cast<size_t>(max_n) * 2 + 15) & ~static_cast<size_t>(15));
+  return (static_cast<size_t>(max_n) * 4 + static_cast<size_t>(max_n) * 2 + 15) & ~static_cast<size_t>(15);
 }
 
+// rank_smem_elems: uint16 slots of shared memory after the bids; an instance
+// whose n*n rank matrix fits there keeps it on chip (small instances), the
+// others use the CTA's slab in global memory.
 template <int kMaxSub>
-__global__ void __launch_bounds__(512) k_batch(BatchInstance *__restrict__ table, const int32_t *__restrict__ order,
+__global__ void __launch_bounds__(512, 2) k_batch(BatchInstance *__restrict__ table, const int32_t *__restrict__ order,
                                                int count, int *queue, uint16_t *__restrict__ slabs,
-                                               size_t slab_elems, int max_n, int dynamic) {
+                                               size_t slab_elems, int max_n, int dynamic, int rank_smem_elems) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint32_t *sbid = reinterpret_cast<uint32_t *>(smem_raw);
   uint16_t *spos = reinterpret_cast<uint16_t *>(smem_raw + static_cast<size_t>(max_n) * 4);
+  uint16_t *srank = reinterpret_cast<uint16_t *>(smem_raw + batch_smem_bytes(max_n));
   __shared__ int s_idx;
   __shared__ int s_next_man;
   __shared__ int s_status;
@@ -53,7 +59,7 @@ __global__ void __launch_bounds__(512) k_batch(BatchInstance *__restrict__ table
   const int lane = tid & 31;
   const int warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
-  uint16_t *rank = slabs + static_cast<size_t>(blockIdx.x) * slab_elems;
+  uint16_t *const slab = slabs + static_cast<size_t>(blockIdx.x) * slab_elems;
 
   for (int round = 0;; ++round) {
     if (tid == 0) s_idx = dynamic ? atomicAdd(queue, 1) : (round == 0 ? static_cast<int>(blockIdx.x) : count);
@@ -72,6 +78,8 @@ __global__ void __launch_bounds__(512) k_batch(BatchInstance *__restrict__ table
       __syncthreads();
       continue;
     }
+    uint16_t *const rank =
+        static_cast<long long>(n) * n <= static_cast<long long>(rank_smem_elems) ? srank : slab;
     for (int w = tid; w < n; w += blockDim.x) sbid[w] = 0xFFFFFFFFu;
     if (tid == 0) {
       s_next_man = 0;
@@ -121,7 +129,8 @@ __global__ void __launch_bounds__(512) k_batch(BatchInstance *__restrict__ table
           pos = 0;
           S = 1;
         }
-        const int rc = man_step<kMaxSub>(bids, keep_going, pref_m, rank, static_cast<const uint32_t *>(nullptr),
+        const int rc = man_step<kMaxSub, true, false>(bids, keep_going, pref_m, static_cast<const uint16_t *>(rank),
+                                                      static_cast<const uint32_t *>(nullptr),
                                          0, n, false, lane, m, pos, S, ahead, settled, hops, bad_value);
         if (rc == kStepMoved || rc == kStepMatchedFree) continue;
         if (rc == kStepBad && lane == 0) s_status = SMP_ERR_INVALID_INPUT;

@@ -124,7 +124,8 @@ int solve_finish(Ctx &c, uint32_t flags, smp_stats *st);
 // batch.cu: the batch kernel on a caller's stream and table (serving loop).
 struct BatchInstance;
 int launch_batch_kernel(Ctx &c, cudaStream_t s, int subs, BatchInstance *table, const int32_t *order, int count,
-                        int *queue, uint16_t *slabs, size_t slab_elems, int max_n, int grid, int block);
+                        int *queue, uint16_t *slabs, size_t slab_elems, int max_n, int grid, int block,
+                        int rank_smem_elems);
 
 // generate.cu
 int generate_side(Ctx &c, int kind, int side, int n, uint64_t seed, uint32_t salt, int param,

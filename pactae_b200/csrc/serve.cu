@@ -153,10 +153,14 @@ void launch_wave(smp_server &s, Wave &w) {
               cudaMemsetAsync(w.queue.ptr, 0, sizeof(int), w.stream) != cudaSuccess))
     rc = c.fail_cuda("wave upload");
   const int block = s.cfg.block_threads > 0 ? s.cfg.block_threads : 512;
+  // 32 KB of shared memory per CTA keeps the rank matrix of requests with
+  // n <= 128 on chip, when it fits beside the bids; the look-ahead is one
+  // window (the batch's best shape on its mix of sizes).
+  const int rank_smem_elems = batch_smem_bytes(max_n) + (32u << 10) <= c.smem_optin ? (16 << 10) : 0;
   if (!rc)
-    rc = launch_batch_kernel(c, w.stream, 8, w.table.as<BatchInstance>(), w.order.as<int32_t>(), count,
+    rc = launch_batch_kernel(c, w.stream, 1, w.table.as<BatchInstance>(), w.order.as<int32_t>(), count,
                              w.queue.as<int>(), w.slabs.as<uint16_t>(), s.slab_elems, max_n,
-                             std::min(count, s.grid), block);
+                             std::min(count, s.grid), block, rank_smem_elems);
   if (!rc && cudaMemcpyAsync(w.h_table, w.table.ptr, sizeof(smp_instance) * count, cudaMemcpyDeviceToHost,
                              w.stream) != cudaSuccess)
     rc = c.fail_cuda("wave readback");

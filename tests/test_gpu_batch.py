@@ -72,3 +72,42 @@ def test_batch_flags_a_bad_instance_only(ctx):
     assert status[4] == pb.SMP_ERR_INVALID_INPUT
     assert st["failed"] == 1
     assert all(s == 0 for i, s in enumerate(status) if i != 4)
+
+
+# -- shapes: the rank matrix on chip or in the slab, tuned or fixed ------------
+@pytest.mark.parametrize("rank_smem_kb", [-1, 32, 96])
+def test_shared_and_global_rank_agree(ctx, rank_smem_kb):
+    # with 32 KB instances up to n = 128 invert into shared memory, with 96 KB
+    # up to n = 221; the rest (and all with -1) use the global slab
+    insts, meta = make_batch(ctx, 40, seed=13, n_lo=16, n_hi=300)
+    with pb.Batch(ctx, insts, rank_smem_kb=rank_smem_kb, tune=False) as batch:
+        cfg = batch.config()
+        assert cfg["rank_smem_kb"] == rank_smem_kb and cfg["tune"] == -1
+        status, props, st = batch.run()
+    assert st["failed"] == 0
+    for (pm, pw, mt), p in zip(insts, props):
+        want, wp = oracle.gs_seq(pm.cpu().numpy(), pw.cpu().numpy())
+        assert np.array_equal(mt.cpu().numpy(), want) and p == wp
+
+
+def test_autotuned_shape(ctx):
+    insts, meta = make_batch(ctx, 64, seed=17, n_lo=16, n_hi=1024)
+    with pb.Batch(ctx, insts) as batch:
+        cfg = batch.config()
+        assert cfg["tune"] == 1
+        assert cfg["block_threads"] in (256, 512) and cfg["ctas_per_sm"] in (1, 2, 4)
+        assert cfg["window"] in (32, 64, 128, 256) and cfg["rank_smem_kb"] in (-1, 32, 64, 96)
+        status, props, st = batch.run()
+    assert st["failed"] == 0
+    for (pm, pw, mt), p in zip(insts, props):
+        want, wst = ctx.solve(pm, pw)
+        assert np.array_equal(mt.cpu().numpy(), want.cpu().numpy()) and p == wst["proposals"]
+
+
+def test_fixed_shape_is_kept(ctx):
+    insts, meta = make_batch(ctx, 20, seed=23, n_lo=16, n_hi=500)
+    with pb.Batch(ctx, insts, block_threads=256, ctas_per_sm=4, window=64, rank_smem_kb=-1) as batch:
+        assert batch.config() == {"block_threads": 256, "ctas_per_sm": 4, "window": 64, "use_graph": 1,
+                                  "rank_smem_kb": -1, "tune": -1}
+        status, props, st = batch.run()
+    assert st["failed"] == 0
