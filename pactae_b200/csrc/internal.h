@@ -84,7 +84,7 @@ struct Ctx {
 
   DeviceBuf d_pref_m, d_pref_w, d_rank, d_prefix, d_bid, d_tailq, d_seen, d_ctrl, d_match;
   DeviceBuf d_husband, d_prank;
-  DeviceBuf d_qcnt, d_qoff, d_qlist;
+  DeviceBuf d_qcnt, d_qlist;
   DeviceBuf gen_keys_a, gen_keys_b, gen_seg, gen_temp, gen_aux;
   Control *h_ctrl = nullptr;  // pinned host copy of the control block
   cudaEvent_t ev[10] = {};

@@ -18,6 +18,8 @@ constexpr int kDefaultTailThreshold = 96;
 constexpr int kDefaultBulkWindow = 256;
 constexpr int kDefaultTailWindow = 256;
 constexpr int kQueryTailWindow = 32;
+// Query buckets hold up to 1.5 K + 32 pairs per woman (at most n).
+int query_capacity(int n, int K) { return std::min(n, K + K / 2 + 32); }
 // Host-pointer solves of at least this n stream their inputs (solve_streamed).
 constexpr int kStreamMinN = 4096;
 constexpr int kRankTailWindow = 256;
@@ -173,21 +175,18 @@ int enqueue_prefix_gather(Ctx &c, int gate) {
 // woman's row (enqueue_qinvert, for all rows or a chunk of them).
 int enqueue_query_index(Ctx &c) {
   const int n = c.n;
+  const int qcap = query_capacity(n, c.K);
   const size_t total = static_cast<size_t>(n) * c.K;
-  int rc = c.d_qcnt.ensure(sizeof(int32_t) * (static_cast<size_t>(n) + 1));
-  if (!rc) rc = c.d_qoff.ensure(sizeof(int32_t) * (static_cast<size_t>(n) + 1));
-  if (!rc) rc = c.d_qlist.ensure(sizeof(uint32_t) * total);
+  int rc = c.d_qcnt.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (!rc) rc = c.d_qlist.ensure(sizeof(uint32_t) * static_cast<size_t>(n) * qcap);
   if (rc) return rc;
-  if (cudaMemsetAsync(c.d_qcnt.ptr, 0, sizeof(int32_t) * (static_cast<size_t>(n) + 1), c.stream) != cudaSuccess)
+  if (cudaMemsetAsync(c.d_qcnt.ptr, 0, sizeof(int32_t) * static_cast<size_t>(n), c.stream) != cudaSuccess)
     return c.fail_cuda("qcnt reset");
-  Control *ctrl = c.d_ctrl.as<Control>();
   const int grid = static_cast<int>(std::min<size_t>(static_cast<size_t>(c.sm_count) * 16, (total + 255) / 256));
-  k_qcount<<<grid, 256, 0, c.stream>>>(c.pref_m, n, c.K, c.d_qcnt.as<int32_t>(), ctrl);
-  k_qscan<<<1, 1024, 0, c.stream>>>(c.d_qcnt.as<int32_t>(), c.d_qoff.as<int32_t>(), n, ctrl);
-  k_qscatter<<<grid, 256, 0, c.stream>>>(c.pref_m, n, c.K, c.d_qoff.as<int32_t>(), c.d_qcnt.as<int32_t>(),
-                                         c.d_qlist.as<uint32_t>(), ctrl);
-  c.launches += 3;
-  return c.check_launch("k_qcount/k_qscan/k_qscatter");
+  k_qscatter<<<grid, 256, 0, c.stream>>>(c.pref_m, n, c.K, qcap, c.d_qcnt.as<int32_t>(), c.d_qlist.as<uint32_t>(),
+                                         c.d_ctrl.as<Control>());
+  c.launches++;
+  return c.check_launch("k_qscatter");
 }
 
 int enqueue_qinvert(Ctx &c, int w0, int w1) {
@@ -201,7 +200,8 @@ int enqueue_qinvert(Ctx &c, int w0, int w1) {
     per_sm = 1;
   }
   const int qgrid = std::max(1, std::min(w1 - w0, c.sm_count * std::max(per_sm, 1)));
-  k_qinvert<<<qgrid, 512, smem, c.stream>>>(c.pref_w, c.n, c.K, c.d_qoff.as<int32_t>(), c.d_qlist.as<uint32_t>(),
+  k_qinvert<<<qgrid, 512, smem, c.stream>>>(c.pref_w, c.n, c.K, query_capacity(c.n, c.K), c.d_qcnt.as<int32_t>(),
+                                            c.d_qlist.as<uint32_t>(),
                                             c.d_prefix.as<uint32_t>(), c.d_ctrl.as<Control>(), w0, w1);
   c.launches++;
   return c.check_launch("k_qinvert");
@@ -705,7 +705,7 @@ void smp_b200_destroy(smp_ctx *ctx) {
     DeviceGuard g(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
     for (DeviceBuf *b : {&c.d_pref_m, &c.d_pref_w, &c.d_rank, &c.d_prefix, &c.d_bid, &c.d_tailq, &c.d_seen,
-                         &c.d_ctrl, &c.d_match, &c.d_husband, &c.d_prank, &c.d_qcnt, &c.d_qoff, &c.d_qlist,
+                         &c.d_ctrl, &c.d_match, &c.d_husband, &c.d_prank, &c.d_qcnt, &c.d_qlist,
                          &c.gen_keys_a, &c.gen_keys_b, &c.gen_seg, &c.gen_temp, &c.gen_aux})
       b->release();
     if (c.copy_stream) cudaStreamSynchronize(c.copy_stream);

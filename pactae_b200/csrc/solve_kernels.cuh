@@ -20,8 +20,8 @@
 //   pref_m, pref_w  int32 [n][n]
 //   rank            RankT [n][n], RankT = uint16_t for n <= 65535, else int32
 //   prefix          uint32 [n][K] = woman << 16 | her rank of the man
-//   qoff, qlist     query index: the (man << 16 | position) pairs naming woman
-//                   w among a man's first K choices are qlist[qoff[w] .. qoff[w+1])
+//   qcnt, qlist     query index: the (man << 16 | position) pairs naming woman
+//                   w among a man's first K choices are qlist[w*qcap ..] (qcnt[w])
 //   bid             u64 [n] (see common.cuh)
 //
 // Every kernel opens with a gate (below) read from the control block, so the
@@ -322,14 +322,17 @@ __global__ void k_prefix(const int32_t *__restrict__ pref_m, const uint16_t *__r
 
 // ---------------------------------------------------------------------------
 // Query mode.  The prefix needs rank_w(m) only for the n*K pairs (w, m) with
-// w among m's first K choices.  k_qcount / k_qscan / k_qscatter bucket those
-// pairs by woman (a counting sort of n*K entries); k_qinvert then streams each
-// woman's row once, inverts it in shared memory and answers her bucket.  The
-// rank matrix is never written: pref_w is read once and nothing n^2-sized is
-// stored.  qcnt is zeroed by the host.
+// w among m's first K choices.  k_qscatter buckets those pairs by woman into
+// fixed-capacity buckets (qlist[w * qcap + i], qcnt[w] of them): qcap =
+// min(n, 1.5 K + 32) is far above the K a woman receives on average, and a
+// bucket that would overflow sets the retry flag, so round 0 stops before any
+// proposal and the rank-mode round solves the instance.  k_qinvert then
+// streams each woman's row once, inverts it in shared memory and answers her
+// bucket.  The rank matrix is never written: pref_w is read once and nothing
+// n^2-sized is stored.  qcnt is zeroed by the host.
 // ---------------------------------------------------------------------------
-__global__ void k_qcount(const int32_t *__restrict__ pref_m, int n, int K, int32_t *__restrict__ qcnt,
-                         Control *ctrl) {
+__global__ void k_qscatter(const int32_t *__restrict__ pref_m, int n, int K, int qcap, int32_t *__restrict__ qcnt,
+                           uint32_t *__restrict__ qlist, Control *ctrl) {
   if (!gate_open(kGateModeQuery, ctrl)) return;
   const size_t total = static_cast<size_t>(n) * K;
   const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
@@ -337,76 +340,25 @@ __global__ void k_qcount(const int32_t *__restrict__ pref_m, int n, int K, int32
     const int m = static_cast<int>(t / K);
     const int r = static_cast<int>(t - static_cast<size_t>(m) * K);
     const int w = __ldg(pref_m + static_cast<size_t>(m) * n + r);
-    if (static_cast<unsigned>(w) < static_cast<unsigned>(n)) {
-      atomicAdd(qcnt + w, 1);
-    } else {
+    if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) {
       report(ctrl, kStatusInvalidInput, w);
+      continue;
     }
-  }
-}
-
-// One CTA of 1024 threads: exclusive scan of qcnt into qoff[0..n], then
-// qcnt is zeroed for use as the fill counter.
-__global__ void __launch_bounds__(1024) k_qscan(int32_t *__restrict__ qcnt, int32_t *__restrict__ qoff, int n,
-                                                Control *ctrl) {
-  if (!gate_open(kGateModeQuery, ctrl)) return;
-  __shared__ int s_warp[32];
-  const int tid = threadIdx.x;
-  const int per = (n + blockDim.x - 1) / blockDim.x;
-  const int lo = min(n, tid * per), hi = min(n, lo + per);
-  int sum = 0;
-  for (int i = lo; i < hi; ++i) sum += qcnt[i];
-  // block-wide exclusive scan of the per-thread sums
-  const int lane = tid & 31, warp = tid >> 5;
-  int x = sum;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const int y = __shfl_up_sync(kFullMask, x, off);
-    if (lane >= off) x += y;
-  }
-  if (lane == 31) s_warp[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    int v = lane < static_cast<int>(blockDim.x >> 5) ? s_warp[lane] : 0;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const int y = __shfl_up_sync(kFullMask, v, off);
-      if (lane >= off) v += y;
+    const int slot = atomicAdd(qcnt + w, 1);
+    if (slot < qcap) {
+      qlist[static_cast<size_t>(w) * qcap + slot] = (static_cast<uint32_t>(m) << 16) | static_cast<uint32_t>(r);
+    } else if (slot == qcap) {
+      atomicExch(&ctrl->retry, 1);  // a bucket overflowed: round 0 stops, the rank-mode round runs
     }
-    s_warp[lane] = v;
-  }
-  __syncthreads();
-  int run = x - sum + (warp > 0 ? s_warp[warp - 1] : 0);
-  for (int i = lo; i < hi; ++i) {
-    const int c = qcnt[i];
-    qoff[i] = run;
-    run += c;
-    qcnt[i] = 0;
-  }
-  if (tid == static_cast<int>(blockDim.x) - 1) qoff[n] = run;
-}
-
-__global__ void k_qscatter(const int32_t *__restrict__ pref_m, int n, int K, const int32_t *__restrict__ qoff,
-                           int32_t *__restrict__ qfill, uint32_t *__restrict__ qlist, Control *ctrl) {
-  if (!gate_open(kGateModeQuery, ctrl)) return;
-  const size_t total = static_cast<size_t>(n) * K;
-  const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
-  for (size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
-    const int m = static_cast<int>(t / K);
-    const int r = static_cast<int>(t - static_cast<size_t>(m) * K);
-    const int w = __ldg(pref_m + static_cast<size_t>(m) * n + r);
-    if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) continue;  // reported by k_qcount
-    const int slot = qoff[w] + atomicAdd(qfill + w, 1);
-    qlist[slot] = (static_cast<uint32_t>(m) << 16) | static_cast<uint32_t>(r);
   }
 }
 
 // Rows [w0, w1) (the whole matrix, or one chunk of it as it arrives).
-__global__ void __launch_bounds__(512) k_qinvert(const int32_t *__restrict__ pref_w, int n, int K,
-                                                 const int32_t *__restrict__ qoff,
+__global__ void __launch_bounds__(512) k_qinvert(const int32_t *__restrict__ pref_w, int n, int K, int qcap,
+                                                 const int32_t *__restrict__ qcnt,
                                                  const uint32_t *__restrict__ qlist,
                                                  uint32_t *__restrict__ prefix, Control *ctrl, int w0, int w1) {
-  if (!gate_open(kGateModeQuery, ctrl)) return;
+  if (!gate_open(kGateModeQuery, ctrl) || ld_volatile_s32(&ctrl->retry)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint16_t *srow = reinterpret_cast<uint16_t *>(smem_raw);
   const int chunks = (n + 7) / 8;
@@ -429,9 +381,10 @@ __global__ void __launch_bounds__(512) k_qinvert(const int32_t *__restrict__ pre
       }
       bad |= any_unset<uint16_t>(v);
     }
-    const int q0 = qoff[w], q1 = qoff[w + 1];
-    for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-      const uint32_t e = qlist[q];
+    const uint32_t *bucket = qlist + static_cast<size_t>(w) * qcap;
+    const int count = min(__ldg(qcnt + w), qcap);
+    for (int q = threadIdx.x; q < count; q += blockDim.x) {
+      const uint32_t e = bucket[q];
       const uint32_t m = e >> 16, r = e & 0xFFFFu;
       prefix[static_cast<size_t>(m) * K + r] = (static_cast<uint32_t>(w) << 16) | srow[m];
     }
@@ -457,6 +410,7 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
                                               unsigned long long *bid, Control *ctrl, int2 *tail_queue, int n,
                                               int tail_threshold, int round) {
   if (!gate_open(round == 0 ? kGateMain : kGateRetry, ctrl)) return;
+  if (round == 0 && ld_volatile_s32(&ctrl->retry)) return;  // a query bucket overflowed
   const bool query = round == 0 && ld_volatile_s32(&ctrl->mode) == kModeQuery;
   const int lane = threadIdx.x & 31;
   // Bring the whole prefix table into L2 (n*K*4 bytes, 23 MB at n = 30000):

@@ -240,3 +240,23 @@ def test_random_instances_against_oracle(ctx, seed):
     want, props = oracle.gs_seq(to_host(pm), to_host(pw))
     assert np.array_equal(to_host(match), want)
     assert st["proposals"] == props
+
+
+def test_query_bucket_overflow_falls_back_to_rank_mode():
+    # Half the men share a first choice with another man (n/2 distinct first
+    # choices: query mode), and every man's next 191 choices are the same
+    # women, so their buckets receive n queries each, far above capacity.
+    n = 2000
+    rng = np.random.default_rng(41)
+    common = np.arange(n - 191, n)
+    pm = np.empty((n, n), np.int32)
+    for m in range(n):
+        first = m % (n // 2)
+        rest = rng.permutation(np.setdiff1d(np.arange(n), np.concatenate([[first], common])))
+        pm[m] = np.concatenate([[first], common, rest])
+    pw = np.stack([rng.permutation(n) for _ in range(n)]).astype(np.int32)
+    want, props = oracle.gs_seq(pm, pw)
+    with pb.Context() as c:
+        match, st = c.solve(pm, pw)
+    assert np.array_equal(match, want) and st["proposals"] == props
+    assert st["mode"] == 2  # query round abandoned, rank-mode round solved it
