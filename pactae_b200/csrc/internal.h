@@ -73,7 +73,8 @@ struct Ctx {
   const int32_t *pref_m = nullptr;  // device pointers the solve reads
   const int32_t *pref_w = nullptr;
   int K = 0;               // prefix width (0 = none)
-  int tail_threshold = 0;  // 0 = tail kernel disabled
+  int tail_threshold = 0;  // 0 = tail kernel disabled; query-mode hand-over
+  int tail_threshold_rank = 0;  // rank-mode hand-over (free women left)
   bool query_ok = false;   // the query mode may be chosen for this n
   int bulk_window = 256;   // look-ahead choices per warp step
   int tail_window = 256;

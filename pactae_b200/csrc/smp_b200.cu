@@ -14,7 +14,8 @@ using namespace smpb200;
 namespace {
 
 constexpr int kDefaultPrefixK = 192;
-constexpr int kDefaultTailThreshold = 96;
+constexpr int kDefaultTailThreshold = 96;      // query mode
+constexpr int kDefaultRankTailThreshold = 32;  // rank mode (deep scans)
 constexpr int kDefaultBulkWindow = 256;
 constexpr int kDefaultTailWindow = 256;
 constexpr int kQueryTailWindow = 32;
@@ -106,6 +107,7 @@ void plan(Ctx &c) {
   c.tail_threshold = 0;
   if (c.tail_threshold_cfg >= 0 && n <= kU16MaxN && tail_smem_bytes(n) <= c.smem_optin)
     c.tail_threshold = c.tail_threshold_cfg > 0 ? c.tail_threshold_cfg : kDefaultTailThreshold;
+  c.tail_threshold_rank = c.tail_threshold_cfg > 0 ? c.tail_threshold_cfg : kDefaultRankTailThreshold;
 }
 
 int enqueue_precheck(Ctx &c, bool allow_perfect) {
@@ -247,7 +249,7 @@ int launch_bulk(Ctx &c, int round) {
   const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
   k_bulk<RankT, kSub><<<resident_grid(c, k_bulk<RankT, kSub>, 256), 256, 0, c.stream>>>(
       c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(), c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
-      c.n, c.tail_threshold, round);
+      c.n, c.tail_threshold, c.tail_threshold > 0 ? std::min(c.tail_threshold, c.tail_threshold_rank) : 0, round);
   c.launches++;
   return c.check_launch("k_bulk");
 }

@@ -408,10 +408,13 @@ template <typename RankT, int kMaxSub>
 __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank,
                                               const uint32_t *__restrict__ prefix, int K,
                                               unsigned long long *bid, Control *ctrl, int2 *tail_queue, int n,
-                                              int tail_threshold, int round) {
+                                              int tail_threshold_query, int tail_threshold_rank, int round) {
   if (!gate_open(round == 0 ? kGateMain : kGateRetry, ctrl)) return;
   if (round == 0 && ld_volatile_s32(&ctrl->retry)) return;  // a query bucket overflowed
   const bool query = round == 0 && ld_volatile_s32(&ctrl->mode) == kModeQuery;
+  // Free women left when the men move to the one-CTA tail: rank-mode
+  // instances scan deep, which many SMs do faster, so they hand over later.
+  const int tail_threshold = query ? tail_threshold_query : tail_threshold_rank;
   const int lane = threadIdx.x & 31;
   // Bring the whole prefix table into L2 (n*K*4 bytes, 23 MB at n = 30000):
   // it was written while pref_w streamed through L2, and every later step of
@@ -586,7 +589,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
       }
       S = 1;
     }
-    const int rc = man_step<kMaxSub, (kMaxSub < 8)>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, ahead, settled,
+    const int rc = man_step<kMaxSub, (kMaxSub < 8), true, (kMaxSub == 8 ? 8 : 1)>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, ahead, settled,
                                      hops, bad_value);
     if (rc == kStepMoved || rc == kStepMatchedFree) continue;
     if (rc == kStepBad) {

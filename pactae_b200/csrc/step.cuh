@@ -181,7 +181,10 @@ __device__ __forceinline__ int try_window(const Bids &bids, int lane, int w, uin
   return -1;
 }
 
-template <int kMaxSub, bool kAhead = true, bool kLdg = true, typename RankT, typename Bids, typename Check>
+// kSReset: the look-ahead (in windows) a man starts with after a move; 1 for
+// chains that end within a few choices, kMaxSub where displaced men scan deep.
+template <int kMaxSub, bool kAhead = true, bool kLdg = true, int kSReset = 1, typename RankT, typename Bids,
+          typename Check>
 __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, const int32_t *__restrict__ pref_m,
                                         const RankT *__restrict__ rank, const uint32_t *__restrict__ prefix, int K,
                                         int n, bool query, int lane, int &m, int &pos, int &S, Ahead &ahead,
@@ -222,7 +225,7 @@ __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, cons
       hops++;
       m = rc == kStepMatchedFree ? -1 : nm;
       pos = np;
-      S = 1;
+      S = kSReset;
       if (kAhead && rc == kStepMoved && next.m == nm && next.pos == np) ahead = next;
       return rc;
     }
@@ -290,7 +293,7 @@ __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, cons
       hops++;
       m = rc == kStepMatchedFree ? -1 : nm;
       pos = np;
-      S = 1;
+      S = kSReset;
       return rc;
     }
     if (rc >= 0) return rc;
