@@ -50,7 +50,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--n", "--size", dest="n", type=int, default=N_DEFAULT)
     ap.add_argument("--kind", type=int, default=0, help="workload kind (0 uniform, 1 congested, 2 correlated)")
     ap.add_argument("--param", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
@@ -83,20 +83,29 @@ def workload_config(args) -> dict:
 # distributed plumbing (replicas only)
 # ---------------------------------------------------------------------------
 class Dist:
+    """One rank of the job (RANK / WORLD_SIZE / LOCAL_RANK from torchrun).
+    The collectives are a barrier and max / sum of a scalar over ranks, on
+    NCCL with a GPU per rank, else on gloo (the CPU tests)."""
+
     def __init__(self, gpus: int):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = "cpu"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                    device_id=torch.device("cuda", self.local_rank))
+            timeout = datetime.timedelta(seconds=120)
+            if torch.cuda.is_available():
+                torch.cuda.set_device(self.local_rank)
+                self.device = f"cuda:{self.local_rank}"
+                dist.init_process_group("nccl", timeout=timeout, device_id=torch.device("cuda", self.local_rank))
+            else:
+                dist.init_process_group("gloo", timeout=timeout)
             self.pg = dist
 
     def _host_only(self, rank: int) -> "Dist":
@@ -104,22 +113,24 @@ class Dist:
         self.rank = rank
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = "cpu"
         return self
 
     def barrier(self):
         if self.pg:
             import torch
 
-            t = torch.ones(1, device=f"cuda:{self.local_rank}")
+            t = torch.ones(1, device=self.device)
             self.pg.all_reduce(t)
-            torch.cuda.synchronize()
+            if self.device != "cpu":
+                torch.cuda.synchronize()
 
     def max(self, v: float) -> float:
         if not self.pg:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local_rank}")
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -128,7 +139,7 @@ class Dist:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local_rank}")
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t)
         return float(t.item())
 
