@@ -53,6 +53,7 @@
 #ifndef SMP_B200_H
 #define SMP_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #if defined(__GNUC__) || defined(__clang__)
@@ -74,7 +75,8 @@ typedef enum smp_status {
   SMP_ERR_TIMEOUT = 5,       /* a bounded device wait ran out               */
   SMP_ERR_BUSY = 6,          /* serving: no slot or HBM budget free          */
   SMP_ERR_NOT_READY = 7,     /* serving: the ticket has not finished         */
-  SMP_ERR_UNSUPPORTED = 8    /* request outside this build's limits          */
+  SMP_ERR_UNSUPPORTED = 8,   /* request outside this build's limits          */
+  SMP_ERR_IO = 9             /* a workload file could not be read or written */
 } smp_status;
 
 /* Largest n accepted by any entry point (rank indices, men and positions are
@@ -238,6 +240,29 @@ SMP_B200_API int smp_b200_solve_batch(smp_ctx *ctx, smp_instance *inst, int32_t 
  * Philox stream as smp_b200_generate.  Host only. */
 SMP_B200_API void smp_b200_batch_instance(uint64_t seed, uint32_t b, int32_t n_lo, int32_t n_hi, int32_t *n_out,
                                           int32_t *kind_out);
+
+/* ------------------------------------------------------------------------ */
+/* The reference's workload text cache (include/utils/generate_workloads_  */
+/* flat.h:283-376, SaveSmpWorkload / LoadSmpWorkload / GetWorkloadFilename): */
+/* "n\n", then the n rows of pref_m and the n rows of pref_w, each row     */
+/* "v v ... v \n".  Host memory, every host thread.                        */
+/* ------------------------------------------------------------------------ */
+
+/* n from a workload file's first line. */
+SMP_B200_API int smp_b200_workload_read_n(const char *path, int32_t *n_out);
+/* Both lists of an n x n workload file into caller buffers (n*n int32 each).
+ * Values are not checked (the solver validates); a short or malformed file
+ * is SMP_ERR_INVALID_INPUT, an unreadable one SMP_ERR_IO.  Replaces
+ * LoadSmpWorkload. */
+SMP_B200_API int smp_b200_workload_read(const char *path, int32_t n, int32_t *pref_m, int32_t *pref_w);
+/* Writes both lists in the same format (replaces SaveSmpWorkload). */
+SMP_B200_API int smp_b200_workload_write(const char *path, const int32_t *pref_m, const int32_t *pref_w,
+                                         int32_t n);
+/* The file name the reference gives a workload of this kind
+ * (SMP_GEN_GROUPED = RANDOM(group_size), SMP_GEN_SOLO, SMP_GEN_REF_CONGESTED,
+ * SMP_GEN_PERFECT), e.g. "smp_workload_random_30000_5.txt".  Replaces
+ * GetWorkloadFilename. */
+SMP_B200_API int smp_b200_workload_filename(int32_t kind, int32_t n, int32_t group_size, char *buf, size_t len);
 
 /* ------------------------------------------------------------------------ */
 /* Serving: a request loop with continuous batching and HBM admission.      */

@@ -156,6 +156,36 @@ def ref() -> ctypes.CDLL:
     return _ref
 
 
+def ref_workload_save(filename: str, pm: np.ndarray, pw: np.ndarray) -> None:
+    """The reference's SaveSmpWorkload: writes data/workloads/<filename>
+    under the current directory."""
+    pm = np.ascontiguousarray(pm, np.int32)
+    pw = np.ascontiguousarray(pw, np.int32)
+    R = ref()
+    R.ref_workload_save.argtypes = [ctypes.c_char_p, _P, _P, ctypes.c_int32]
+    assert R.ref_workload_save(filename.encode(), pm.ctypes.data, pw.ctypes.data, pm.shape[0]) == 0
+
+
+def ref_workload_load(filename: str, n: int) -> tuple[np.ndarray, np.ndarray]:
+    """The reference's LoadSmpWorkload on data/workloads/<filename>."""
+    pm = np.empty((n, n), np.int32)
+    pw = np.empty((n, n), np.int32)
+    R = ref()
+    R.ref_workload_load.argtypes = [ctypes.c_char_p, ctypes.c_int32, _P, _P]
+    assert R.ref_workload_load(filename.encode(), n, pm.ctypes.data, pw.ctypes.data) == 0
+    return pm, pw
+
+
+def ref_workload_filename(workload_type: int, n: int, group_size: int) -> str:
+    """The reference's GetWorkloadFilename (WorkloadType: PERFECT 0, RANDOM 1,
+    CONGESTED 2, SOLO 3)."""
+    buf = ctypes.create_string_buffer(256)
+    R = ref()
+    R.ref_workload_filename.argtypes = [ctypes.c_int, ctypes.c_int32, ctypes.c_int32, ctypes.c_char_p, ctypes.c_int32]
+    assert R.ref_workload_filename(workload_type, n, group_size, buf, len(buf)) == 0
+    return buf.value.decode()
+
+
 def ref_threads() -> int:
     return int(ref().ref_threads())
 

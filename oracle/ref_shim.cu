@@ -20,6 +20,7 @@
 #include "smp/smp_engine_gs_2.h"
 #include "smp/smp_engine_mw_1.h"
 #include "smp/smp_engine_mw_2.h"
+#include "utils/generate_workloads_flat.h"
 
 namespace {
 
@@ -124,5 +125,31 @@ int ref_threads(void) { return hw_threads(); }
 
 /* 1 if the engine can run at this n without the out-of-range writes above. */
 int ref_engine_safe(int engine, int32_t n) { return engine_safe(engine, n) ? 1 : 0; }
+
+// The reference's workload cache (generate_workloads_flat.h:283-376).  Both
+// prepend "data/workloads/" to the file name, relative to the working
+// directory, as the reference does.
+int ref_workload_save(const char *filename, const int32_t *pref_m, const int32_t *pref_w, int32_t n) {
+  const size_t nn = static_cast<size_t>(n) * n;
+  FlatPreferenceList m(pref_m, pref_m + nn), w(pref_w, pref_w + nn);
+  SaveSmpWorkload(filename, m, w, n);
+  return 0;
+}
+int ref_workload_load(const char *filename, int32_t n, int32_t *pref_m, int32_t *pref_w) {
+  FlatPreferenceList m, w;
+  int n_file = 0;
+  LoadSmpWorkload(filename, m, w, n_file);
+  if (n_file != n) return -1;
+  std::memcpy(pref_m, m.data(), sizeof(int32_t) * m.size());
+  std::memcpy(pref_w, w.data(), sizeof(int32_t) * w.size());
+  return 0;
+}
+int ref_workload_filename(int type, int32_t n, int32_t group_size, char *buf, int32_t len) {
+  const String name = GetWorkloadFilename(static_cast<WorkloadType>(type), static_cast<size_t>(n),
+                                          static_cast<size_t>(group_size));
+  if (static_cast<int32_t>(name.size()) + 1 > len) return -1;
+  std::memcpy(buf, name.c_str(), name.size() + 1);
+  return 0;
+}
 
 }  // extern "C"

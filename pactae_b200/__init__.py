@@ -13,6 +13,7 @@ Every solve runs in libsmp_b200.so on the GPU; there is no CPU path.
 from __future__ import annotations
 
 import ctypes
+import os
 import time
 from typing import Any
 
@@ -26,6 +27,7 @@ from ._lib import (  # noqa: F401  (re-exported constants)
     SMP_ERR_CUDA,
     SMP_ERR_INVALID_ARG,
     SMP_ERR_INVALID_INPUT,
+    SMP_ERR_IO,
     SMP_ERR_NOT_READY,
     SMP_ERR_OOM,
     SMP_ERR_TIMEOUT,
@@ -260,6 +262,33 @@ class Context:
         _check(lib.smp_b200_generate(self.handle, kind, n, seed, salt, param, _ptr(pm), _ptr(pw), 0),
                "smp_b200_generate")
         return pm, pw
+
+
+# -- the reference's workload text cache (generate_workloads_flat.h:283-376) ----
+def read_workload(path) -> tuple[np.ndarray, np.ndarray]:
+    """(pref_m, pref_w) of a workload file in the reference's format
+    (LoadSmpWorkload): "n", then n rows of each list."""
+    n = ctypes.c_int32()
+    _check(lib.smp_b200_workload_read_n(os.fsencode(path), ctypes.byref(n)), "smp_b200_workload_read_n")
+    pm = np.empty((n.value, n.value), dtype=np.int32)
+    pw = np.empty((n.value, n.value), dtype=np.int32)
+    _check(lib.smp_b200_workload_read(os.fsencode(path), n.value, _ptr(pm), _ptr(pw)), "smp_b200_workload_read")
+    return pm, pw
+
+
+def write_workload(path, pref_m: Any, pref_w: Any) -> None:
+    """Writes both lists in the reference's format (SaveSmpWorkload)."""
+    pm = _host_array(pref_m)
+    pw = _host_array(pref_w)
+    n = pm.shape[0] if pm.ndim == 2 else int(round(pm.size ** 0.5))
+    _check(lib.smp_b200_workload_write(os.fsencode(path), _ptr(pm), _ptr(pw), n), "smp_b200_workload_write")
+
+
+def workload_filename(kind: int, n: int, group_size: int = 5) -> str:
+    """The file name the reference gives a generated workload (GetWorkloadFilename)."""
+    buf = ctypes.create_string_buffer(128)
+    _check(lib.smp_b200_workload_filename(kind, n, group_size, buf, len(buf)), "smp_b200_workload_filename")
+    return buf.value.decode()
 
 
 def batch_instance(seed: int, b: int, n_lo: int, n_hi: int) -> tuple[int, int]:

@@ -21,6 +21,7 @@ SMP_ERR_TIMEOUT = 5
 SMP_ERR_BUSY = 6
 SMP_ERR_NOT_READY = 7
 SMP_ERR_UNSUPPORTED = 8
+SMP_ERR_IO = 9
 
 SMP_B200_MAX_N = 1048575
 SMP_B200_STATIC_MAX_N = 1024
@@ -60,6 +61,7 @@ ABI_SYMBOLS = (
     "smp_b200_batch_run",
     "smp_b200_batch_run_plain",
     "smp_b200_batch_destroy", "smp_b200_batch_config",
+    "smp_b200_workload_read_n", "smp_b200_workload_read", "smp_b200_workload_write", "smp_b200_workload_filename",
     "smp_b200_solve_batch",
     "smp_b200_batch_instance",
     "smp_b200_server_create",
@@ -220,6 +222,11 @@ _SIGNATURES = {
     "smp_b200_batch_run_plain": (ctypes.c_int, [_P, ctypes.POINTER(smp_instance), ctypes.POINTER(smp_batch_stats)]),
     "smp_b200_batch_destroy": (None, [_P]),
     "smp_b200_batch_config": (ctypes.c_int, [_P, ctypes.POINTER(smp_batch_cfg)]),
+    "smp_b200_workload_read_n": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32)]),
+    "smp_b200_workload_read": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, _P, _P]),
+    "smp_b200_workload_write": (ctypes.c_int, [ctypes.c_char_p, _P, _P, ctypes.c_int32]),
+    "smp_b200_workload_filename": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_char_p,
+                                                  ctypes.c_size_t]),
     "smp_b200_solve_batch": (ctypes.c_int, [_P, ctypes.POINTER(smp_instance), _I32, ctypes.POINTER(smp_batch_cfg),
                                             ctypes.POINTER(smp_batch_stats)]),
     "smp_b200_batch_instance": (None, [_U64, _U32, _I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),

@@ -32,7 +32,7 @@ NVCC_FLAGS = [
     "-Xptxas", "-warn-spills",
 ]
 
-SOURCES = ["smp_b200.cu", "generate.cu", "batch.cu", "serve.cu", "static_solve.cu"]
+SOURCES = ["smp_b200.cu", "generate.cu", "batch.cu", "serve.cu", "static_solve.cu", "workload_io.cpp"]
 
 
 def _nvcc() -> str:
@@ -43,7 +43,7 @@ def _nvcc() -> str:
 
 
 def _inputs() -> list[Path]:
-    files = [p for p in CSRC.iterdir() if p.suffix in (".cu", ".cuh", ".h")]
+    files = [p for p in CSRC.iterdir() if p.suffix in (".cu", ".cuh", ".h", ".cpp")]
     files += [p for p in INCLUDE.iterdir() if p.suffix == ".h"]
     files.append(Path(__file__))
     return files

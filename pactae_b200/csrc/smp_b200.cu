@@ -18,7 +18,6 @@ constexpr int kDefaultTailThreshold = 96;      // query mode
 constexpr int kDefaultRankTailThreshold = 32;  // rank mode (deep scans)
 constexpr int kDefaultBulkWindow = 256;
 constexpr int kDefaultTailWindow = 256;
-constexpr int kQueryTailWindow = 32;
 // Query buckets hold up to 1.5 K + 32 pairs per woman (at most n).
 int query_capacity(int n, int K) { return std::min(n, K + K / 2 + 32); }
 // Host-pointer solves of at least this n stream their inputs (solve_streamed).
@@ -647,6 +646,7 @@ const char *smp_b200_strerror(int status) {
     case SMP_ERR_BUSY: return "no slot or HBM budget free";
     case SMP_ERR_NOT_READY: return "not finished yet";
     case SMP_ERR_UNSUPPORTED: return "unsupported request";
+    case SMP_ERR_IO: return "a workload file could not be read or written";
     default: return "unknown status";
   }
 }
