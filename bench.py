@@ -53,6 +53,9 @@ def parse_args():
     ap.add_argument("--n", "--size", dest="n", type=int, default=N_DEFAULT)
     ap.add_argument("--kind", type=int, default=0, help="workload kind (0 uniform, 1 congested, 2 correlated)")
     ap.add_argument("--param", type=int, default=0)
+    ap.add_argument("--init-study", action="store_true",
+                    help="the reference's init study (benchmark/figure_5.cu): its GPU init engine beside ours")
+    ap.add_argument("--init-sizes", default="1000,5000,10000,15000,30000")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 8192-instance batched leg")
@@ -599,8 +602,68 @@ def run_reference(args, dist: Dist) -> dict | None:
     }
 
 
+def run_init_study(args) -> None:
+    """The reference's init study (benchmark/figure_5.cu) on this GPU: its GPU
+    init engine Smp-Init-Gpu (SmpInitEngine3, built from its headers into
+    oracle/_ref/libsmpref_gpu.so with its release flags) beside this
+    library's inversion (smp_b200_invert, the same int32 rank matrix), on the
+    reference's CONGESTED workload at n = 1000 .. 30000.  The reference's
+    figures are its own report (kernel time = its stopwatch minus its
+    transfers); ours are CUDA events around the inversion kernel.  One JSON
+    line per n."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import oracle
+    import pactae_b200 as pb
+
+    lib_path = ROOT / "oracle" / "_ref" / "libsmpref_gpu.so"
+    if not lib_path.exists():
+        print(json.dumps({"init_study": "unavailable", "why": "oracle/_ref/libsmpref_gpu.so not built"}))
+        return
+    R = ctypes.CDLL(str(lib_path))
+    dbl = ctypes.POINTER(ctypes.c_double)
+    R.ref_gpu_init.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int, dbl, dbl, dbl]
+    ctx = pb.Context(0)
+    for n in [int(x) for x in args.init_sizes.split(",")]:
+        pm, pw = oracle.generate(pb.SMP_GEN_REF_CONGESTED, n, SEED)
+        ref = {}
+        for pr in (0, 1):
+            runs = []
+            for _ in range(4):  # the first run warms the engine up; the best of the other three is kept
+                k, t, tot = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+                rc = R.ref_gpu_init(pm.ctypes.data, pw.ctypes.data, n, pr, ctypes.byref(k), ctypes.byref(t),
+                                    ctypes.byref(tot))
+                runs.append((k.value, t.value, tot.value, rc))
+            k, t, tot, rc = min(runs[1:])
+            ref["rank_and_pr" if pr else "rank"] = {"kernel_ms": round(k, 3), "transfer_ms": round(t, 3),
+                                                     "total_ms": round(tot, 3), "status": rc}
+        dpw = torch.from_numpy(pw).cuda()
+        ctx.invert(dpw)  # warm-up
+        times = []
+        for _ in range(3):
+            rank = ctx.invert(dpw)
+            times.append(ctx.stats()["init_ms"])
+        ours = min(times)
+        if n <= 5000:
+            assert np.array_equal(rank.cpu().numpy(), oracle.invert(pw)), "rank matrix differs from the oracle"
+        print(json.dumps({"init_study": "CONGESTED (reference generate_workloads_flat.h:14-47)", "n": n,
+                          "reference_smp_init_gpu": ref,
+                          "ours_k_invert_ms": round(ours, 4),
+                          "rank_kernel_speedup": round(ref["rank"]["kernel_ms"] / ours, 1) if ours > 0 else None,
+                          "ours_bytes_per_s": round(8 * n * n / (ours * 1e-3) / 1e9, 1)}), flush=True)
+        del dpw, rank
+        torch.cuda.empty_cache()
+    ctx.close()
+
+
 def main():
     args = parse_args()
+    if args.init_study:
+        run_init_study(args)
+        return
     if args.impl == "reference":
         # Host-only arm: rank 0 times the reference's CPU engine; other ranks
         # exit without work and no process group is needed.

@@ -89,6 +89,8 @@ def build_oracle(verbose: bool = False) -> None:
     ref = Path(os.environ.get("SMP_REFERENCE_DIR", "/root/reference"))
     if (ref / "src" / "smp" / "smp_engine_gs_1.cu").exists():
         targets.append("ref")
+    if (ref / "include" / "smp" / "smp_init_3.h").exists():
+        targets.append("ref-gpu")
     cmd = ["make", "-s", "-C", str(oracle), *targets, f"REF={ref}"]
     if verbose:
         print(" ".join(cmd), flush=True)

@@ -4,6 +4,7 @@
 // solve_kernels.cuh and generate.cu.
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 
 #include "common.cuh"
 #include "internal.h"
@@ -129,6 +130,23 @@ int enqueue_precheck(Ctx &c, bool allow_perfect) {
 template <typename RankT>
 int enqueue_invert(Ctx &c, const int32_t *pref_w, RankT *rank, int gate) {
   const int n = c.n;
+  if constexpr (std::is_same<RankT, int32_t>::value) {
+    const size_t smem16 = row_smem_bytes<uint16_t>(n);
+    if (n <= kU16MaxN && smem16 <= c.smem_optin) {  // int32 output from a uint16 shared row
+      if (cudaFuncSetAttribute(k_invert_wide, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem16)) != cudaSuccess)
+        return c.fail_cuda("k_invert_wide smem attribute");
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_invert_wide, 512, smem16) != cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 1;
+      }
+      const int grid = std::min(n, c.sm_count * std::max(per_sm, 1));
+      k_invert_wide<<<grid, 512, smem16, c.stream>>>(pref_w, rank, n, c.d_ctrl.as<Control>(), gate);
+      c.launches++;
+      return c.check_launch("k_invert_wide");
+    }
+  }
   const size_t smem = row_smem_bytes<RankT>(n);
   if (smem <= c.smem_optin) {
     if (cudaFuncSetAttribute(k_invert<RankT>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -231,6 +231,48 @@ __global__ void __launch_bounds__(512) k_invert(const int32_t *__restrict__ pref
   if (bad) report(ctrl, kStatusInvalidInput, -1);
 }
 
+// int32 ranks (the reference's layout, smp_b200_invert) from a uint16
+// shared row: ranks below 65536 fit 16 bits, so the row takes half the
+// shared memory of an int32 one (three CTAs per SM at n = 30000 instead of
+// one).  Each 16-byte output chunk is widened from 8 bytes of the row, which
+// sits at the output row's offset from a 16-byte boundary.
+__global__ void __launch_bounds__(512) k_invert_wide(const int32_t *__restrict__ pref_w, int32_t *__restrict__ rank,
+                                                     int n, Control *ctrl, int gate) {
+  if (!gate_open(gate, ctrl)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint16_t *sbuf = reinterpret_cast<uint16_t *>(smem_raw);
+  bool bad = false;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    int32_t *out = rank + static_cast<size_t>(w) * n;
+    const int pre = static_cast<int>((reinterpret_cast<uintptr_t>(out) & 15u) / sizeof(int32_t));
+    const int chunks = (pre + n + 3) / 4;                   // 16-byte output chunks
+    load_row(pref_w + static_cast<size_t>(w) * n, sbuf, sbuf + pre, (pre + n + 7) / 8, n, bad);
+    const uint2 *s2 = reinterpret_cast<const uint2 *>(sbuf);
+    uint4 *o4 = reinterpret_cast<uint4 *>(reinterpret_cast<uintptr_t>(out) -
+                                          static_cast<uintptr_t>(pre) * sizeof(int32_t));
+    for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
+      const uint2 v = s2[c];
+      const uint32_t vals[4] = {v.x & 0xFFFFu, v.x >> 16, v.y & 0xFFFFu, v.y >> 16};
+      const int first = c * 4 - pre;  // row element in the chunk's first slot
+      if (first >= 0 && first + 4 <= n) {
+        bad |= (__vcmpeq2(v.x, 0xFFFFFFFFu) | __vcmpeq2(v.y, 0xFFFFFFFFu)) != 0;
+        __stcs(o4 + c, make_uint4(vals[0], vals[1], vals[2], vals[3]));
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int e = first + k;
+          if (e >= 0 && e < n) {
+            bad |= (vals[k] == 0xFFFFu);
+            __stcs(out + e, static_cast<int32_t>(vals[k]));
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (bad) report(ctrl, kStatusInvalidInput, -1);
+}
+
 // Inversion for rows that do not fit in shared memory: scatter straight to
 // global memory, then verify rank[w][pref_w[w][r]] == r in a second pass.
 __global__ void k_invert_global(const int32_t *__restrict__ pref_w, int32_t *__restrict__ rank, int n,
