@@ -280,7 +280,9 @@ typedef struct smp_server_cfg {
                            /* matrices (10 n^2 per request); 0 = 64 GiB              */
   int32_t block_threads;   /* threads per CTA of the batched launches; 0 = 512       */
   int32_t ctas_per_sm;     /* CTAs per SM of a batched launch; 0 = 2                 */
-  uint64_t reserved[3];
+  uint64_t large_slots;    /* requests above route_n solved at once, each on its own */
+                           /* context and stream; 0 = 4 (at most 16)                 */
+  uint64_t reserved[2];
 } smp_server_cfg;
 
 typedef struct smp_result {

@@ -382,7 +382,7 @@ class Server:
     copied in when admitted and the matching copied back."""
 
     def __init__(self, device: int = 0, max_wave: int = 0, route_n: int = 0, waves: int = 0, hbm_budget: int = 0,
-                 block_threads: int = 0, ctas_per_sm: int = 0):
+                 block_threads: int = 0, ctas_per_sm: int = 0, large_slots: int = 0):
         cfg = smp_server_cfg()
         cfg.device = device
         cfg.max_wave = max_wave
@@ -391,6 +391,7 @@ class Server:
         cfg.hbm_budget = hbm_budget
         cfg.block_threads = block_threads
         cfg.ctas_per_sm = ctas_per_sm
+        cfg.large_slots = large_slots
         handle = ctypes.c_void_p()
         _check(lib.smp_b200_server_create(ctypes.byref(cfg), ctypes.byref(handle)), "smp_b200_server_create")
         self._h = handle

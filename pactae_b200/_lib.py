@@ -163,7 +163,8 @@ class smp_server_cfg(ctypes.Structure):
         ("hbm_budget", ctypes.c_uint64),
         ("block_threads", ctypes.c_int32),
         ("ctas_per_sm", ctypes.c_int32),
-        ("reserved", ctypes.c_uint64 * 3),
+        ("large_slots", ctypes.c_uint64),
+        ("reserved", ctypes.c_uint64 * 2),
     ]
 
 

@@ -5,8 +5,10 @@
 //     launch of the batch kernel (one CTA per request) on its own stream, and
 //     several waves are in flight at once, so a request that arrives while
 //     others run starts in the next wave without waiting for them;
-//   - larger requests go through the all-SM single-instance pipeline on its
-//     own context and stream, concurrently with the waves.
+//   - larger requests go through the single-instance pipeline, several at
+//     once (large_slots contexts, each with its own stream): one solve's
+//     latency-bound chains and one-SM tail leave most SMs to the others
+//     and to the waves.
 // A request is admitted when its matrices (two n x n int32 lists and the
 // n x n uint16 rank matrix: 10 n^2 bytes) fit in the budget; it releases
 // them when it completes.  The reference has no serving layer.
@@ -68,7 +70,12 @@ struct Wave {
 struct smp_server {
   smp_server_cfg cfg = {};
   smp_ctx *ctx = nullptr;        // device, sm count, error text for the waves
-  smp_ctx *large_ctx = nullptr;  // all-SM pipeline
+  struct LargeSlot {
+    smp_ctx *ctx = nullptr;  // single-instance pipeline
+    cudaEvent_t done = nullptr;
+    Request *running = nullptr;
+  };
+  std::vector<LargeSlot> large;
   std::thread thread;
   std::mutex mu;
   std::condition_variable cv_submit, cv_done;
@@ -80,8 +87,6 @@ struct smp_server {
   // server-thread state
   std::deque<Request *> pending, small_q, large_q;
   std::vector<Wave> waves;
-  Request *large_running = nullptr;
-  cudaEvent_t large_done = nullptr;
   uint64_t used = 0;
   int grid = 0;
   size_t slab_elems = 0;
@@ -184,32 +189,32 @@ void reap_wave(smp_server &s, Wave &w) {
   w.busy = false;
 }
 
-void launch_large(smp_server &s) {
+void launch_large(smp_server &s, smp_server::LargeSlot &slot) {
   Request *r = s.large_q.front();
   s.large_q.pop_front();
-  Ctx &lc = s.large_ctx->c;
+  Ctx &lc = slot.ctx->c;
   r->t_launch = Clock::now();
   int rc = stage_request(r, lc.stream);
   if (!rc) rc = solve_enqueue(lc, r->dev_pm(), r->dev_pw(), r->n, r->dev_match(), SMP_F_DEVICE_PTRS);
   if (!rc) rc = unstage_request(r, lc.stream);
-  if (!rc && cudaEventRecord(s.large_done, lc.stream) != cudaSuccess) rc = lc.fail_cuda("large event");
+  if (!rc && cudaEventRecord(slot.done, lc.stream) != cudaSuccess) rc = lc.fail_cuda("large event");
   if (rc) {
     cudaStreamSynchronize(lc.stream);
     finish(s, r, rc, 0);
     return;
   }
-  s.large_running = r;
+  slot.running = r;
   std::lock_guard<std::mutex> lock(s.mu);
   s.stats.large++;
 }
 
-void reap_large(smp_server &s) {
-  if (!s.large_running || cudaEventQuery(s.large_done) != cudaSuccess) return;
-  Ctx &lc = s.large_ctx->c;
+void reap_large(smp_server &s, smp_server::LargeSlot &slot) {
+  if (!slot.running || cudaEventQuery(slot.done) != cudaSuccess) return;
+  Ctx &lc = slot.ctx->c;
   smp_stats st = {};
   const int rc = solve_finish(lc, SMP_F_DEVICE_PTRS, &st);
-  finish(s, s.large_running, rc, rc == SMP_OK ? st.proposals : 0);
-  s.large_running = nullptr;
+  finish(s, slot.running, rc, rc == SMP_OK ? st.proposals : 0);
+  slot.running = nullptr;
 }
 
 void server_loop(smp_server *sp) {
@@ -219,8 +224,10 @@ void server_loop(smp_server *sp) {
   for (;;) {
     {
       std::unique_lock<std::mutex> lock(s.mu);
-      const bool idle = s.pending.empty() && s.small_q.empty() && s.large_q.empty() && !s.large_running &&
-                        std::none_of(s.waves.begin(), s.waves.end(), [](const Wave &w) { return w.busy; });
+      const bool idle =
+          s.pending.empty() && s.small_q.empty() && s.large_q.empty() &&
+          std::none_of(s.large.begin(), s.large.end(), [](const smp_server::LargeSlot &l) { return l.running; }) &&
+          std::none_of(s.waves.begin(), s.waves.end(), [](const Wave &w) { return w.busy; });
       if (idle) s.cv_submit.wait_for(lock, std::chrono::microseconds(200), [&] { return s.stop || !s.submitted.empty(); });
       while (!s.submitted.empty()) {
         s.pending.push_back(s.submitted.front());
@@ -239,7 +246,8 @@ void server_loop(smp_server *sp) {
       s.stats.admitted_bytes = static_cast<int64_t>(s.used);
       s.stats.peak_bytes = std::max<int64_t>(s.stats.peak_bytes, static_cast<int64_t>(s.used));
     }
-    if (!s.large_running && !s.large_q.empty()) launch_large(s);
+    for (auto &slot : s.large)
+      if (!slot.running && !s.large_q.empty()) launch_large(s, slot);
     for (Wave &w : s.waves) {
       if (w.busy || s.small_q.empty()) continue;
       while (!s.small_q.empty() && static_cast<int>(w.reqs.size()) < max_wave) {
@@ -249,7 +257,7 @@ void server_loop(smp_server *sp) {
       launch_wave(s, w);
     }
     for (Wave &w : s.waves) reap_wave(s, w);
-    reap_large(s);
+    for (auto &slot : s.large) reap_large(s, slot);
     // short pause while work is on the device
     std::this_thread::sleep_for(std::chrono::microseconds(20));
   }
@@ -269,8 +277,10 @@ void destroy_server(smp_server *s) {
     w.queue.release();
     w.slabs.release();
   }
-  if (s->large_done) cudaEventDestroy(s->large_done);
-  if (s->large_ctx) smp_b200_destroy(s->large_ctx);
+  for (auto &slot : s->large) {
+    if (slot.done) cudaEventDestroy(slot.done);
+    if (slot.ctx) smp_b200_destroy(slot.ctx);
+  }
   if (s->ctx) smp_b200_destroy(s->ctx);
   for (auto &kv : s->tickets) delete kv.second;
   delete s;
@@ -293,7 +303,9 @@ int smp_b200_server_create(const smp_server_cfg *cfg, smp_server **out) {
   smp_cfg c1 = {};
   c1.device = s->cfg.device;
   int rc = smp_b200_create(&s->ctx, &c1);
-  if (!rc) rc = smp_b200_create(&s->large_ctx, &c1);
+  s->large.resize(static_cast<size_t>(s->cfg.large_slots > 0 ? std::min<uint64_t>(s->cfg.large_slots, 16) : 4));
+  for (auto &slot : s->large)
+    if (!rc) rc = smp_b200_create(&slot.ctx, &c1);
   if (rc) {
     destroy_server(s);
     return rc;
@@ -317,7 +329,8 @@ int smp_b200_server_create(const smp_server_cfg *cfg, smp_server **out) {
       rc = SMP_ERR_OOM;
     if (rc) break;
   }
-  if (!rc && cudaEventCreateWithFlags(&s->large_done, cudaEventDisableTiming) != cudaSuccess) rc = SMP_ERR_CUDA;
+  for (auto &slot : s->large)
+    if (!rc && cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming) != cudaSuccess) rc = SMP_ERR_CUDA;
   if (rc) {
     cudaGetLastError();
     destroy_server(s);

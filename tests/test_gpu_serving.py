@@ -25,11 +25,13 @@ def make_requests(ctx, count, seed, n_lo, n_hi):
     return reqs
 
 
-def test_results_alone_equal_results_in_the_mix(ctx):
+@pytest.mark.parametrize("large_slots", [1, 3])
+def test_results_alone_equal_results_in_the_mix(ctx, large_slots):
     reqs = make_requests(ctx, 40, seed=6, n_lo=64, n_hi=3000)
     alone = [ctx.solve(pm, pw) for pm, pw, _ in reqs]
-    # route_n = 1024: the larger requests take the all-SM pipeline alongside the waves
-    with pb.Server(route_n=1024, max_wave=8, waves=3) as srv:
+    # route_n = 1024: the larger requests take the single-instance pipeline
+    # (large_slots of them at once) alongside the waves
+    with pb.Server(route_n=1024, max_wave=8, waves=3, large_slots=large_slots) as srv:
         tickets = [srv.submit(pm, pw, mt) for pm, pw, mt in reqs]
         results = [srv.poll(t) for t in tickets]
         st = srv.stats()
