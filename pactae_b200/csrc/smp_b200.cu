@@ -178,12 +178,34 @@ int enqueue_invert_any(Ctx &c, int gate) {
                            : enqueue_invert<int32_t>(c, c.pref_w, c.d_rank.as<int32_t>(), gate);
 }
 
+// The rank matrix a solve's proposals read: inverted (woman-major, kept for
+// the checker) and transposed to man-major (d_rankT).
+int enqueue_rank(Ctx &c, int gate) {
+  int rc = c.d_rankT.ensure(static_cast<size_t>(c.n) * c.n * c.rank_bytes);
+  if (!rc) rc = enqueue_invert_any(c, gate);
+  if (rc) return rc;
+  const int tiles = (c.n + 63) / 64;
+  const int grid = static_cast<int>(std::min<long long>(static_cast<long long>(c.sm_count) * 4,
+                                                        static_cast<long long>(tiles) * tiles));
+  if (c.rank_bytes == 2 && c.n % 2 == 0)
+    k_transpose_u16x2<<<grid, 512, 0, c.stream>>>(c.d_rank.as<uint16_t>(), c.d_rankT.as<uint16_t>(), c.n,
+                                                  c.d_ctrl.as<Control>(), gate);
+  else if (c.rank_bytes == 2)
+    k_transpose<uint16_t><<<grid, 512, 0, c.stream>>>(c.d_rank.as<uint16_t>(), c.d_rankT.as<uint16_t>(), c.n,
+                                                      c.d_ctrl.as<Control>(), gate);
+  else
+    k_transpose<int32_t><<<grid, 512, 0, c.stream>>>(c.d_rank.as<int32_t>(), c.d_rankT.as<int32_t>(), c.n,
+                                                     c.d_ctrl.as<Control>(), gate);
+  c.launches++;
+  return c.check_launch("k_transpose");
+}
+
 int enqueue_prefix_gather(Ctx &c, int gate) {
   if (c.K <= 0) return SMP_OK;
   const int n = c.n;
   const size_t total = static_cast<size_t>(n) * c.K;
   const int grid = static_cast<int>(std::min<size_t>(static_cast<size_t>(c.sm_count) * 16, (total + 255) / 256));
-  k_prefix<<<grid, 256, 0, c.stream>>>(c.pref_m, c.d_rank.as<uint16_t>(), c.d_prefix.as<uint32_t>(), n, c.K,
+  k_prefix<<<grid, 256, 0, c.stream>>>(c.pref_m, c.d_rankT.as<uint16_t>(), c.d_prefix.as<uint32_t>(), n, c.K,
                                        c.d_ctrl.as<Control>(), gate);
   c.launches++;
   return c.check_launch("k_prefix");
@@ -254,7 +276,7 @@ int enqueue_init(Ctx &c) {
     rc = enqueue_query(c);
     if (rc) return rc;
   }
-  rc = enqueue_invert_any(c, kGateModeRank);
+  rc = enqueue_rank(c, kGateModeRank);
   if (rc) return rc;
   if (cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
   return enqueue_prefix_gather(c, kGateModeRank);
@@ -262,7 +284,7 @@ int enqueue_init(Ctx &c) {
 
 template <typename RankT, int kSub>
 int launch_bulk(Ctx &c, int round) {
-  const RankT *rank = reinterpret_cast<const RankT *>(c.d_rank.ptr);
+  const RankT *rank = reinterpret_cast<const RankT *>(c.d_rankT.ptr);  // man-major
   const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
   k_bulk<RankT, kSub><<<resident_grid(c, k_bulk<RankT, kSub>, 256), 256, 0, c.stream>>>(
       c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(), c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
@@ -273,7 +295,7 @@ int launch_bulk(Ctx &c, int round) {
 
 template <typename RankT, int kSub>
 int launch_tail(Ctx &c, int round, int only_mode) {
-  const RankT *rank = reinterpret_cast<const RankT *>(c.d_rank.ptr);
+  const RankT *rank = reinterpret_cast<const RankT *>(c.d_rankT.ptr);  // man-major
   const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
   const size_t smem = tail_smem_bytes(c.n);
   if (cudaFuncSetAttribute(k_tail<RankT, kSub>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -335,7 +357,7 @@ int enqueue_retry_round(Ctx &c) {
   k_retry_reset<<<1, 1024, 0, c.stream>>>(c.d_bid.as<unsigned long long>(), c.n, c.d_ctrl.as<Control>());
   c.launches++;
   int rc = c.check_launch("k_retry_reset");
-  if (!rc) rc = enqueue_invert_any(c, kGateRetry);
+  if (!rc) rc = enqueue_rank(c, kGateRetry);
   if (!rc) rc = enqueue_prefix_gather(c, kGateRetry);
   if (!rc) rc = enqueue_round<RankT>(c, 1);
   return rc;
@@ -724,7 +746,7 @@ void smp_b200_destroy(smp_ctx *ctx) {
   {
     DeviceGuard g(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
-    for (DeviceBuf *b : {&c.d_pref_m, &c.d_pref_w, &c.d_rank, &c.d_prefix, &c.d_bid, &c.d_tailq, &c.d_seen,
+    for (DeviceBuf *b : {&c.d_pref_m, &c.d_pref_w, &c.d_rank, &c.d_rankT, &c.d_prefix, &c.d_bid, &c.d_tailq, &c.d_seen,
                          &c.d_ctrl, &c.d_match, &c.d_husband, &c.d_prank, &c.d_qcnt, &c.d_qlist,
                          &c.gen_keys_a, &c.gen_keys_b, &c.gen_seg, &c.gen_temp, &c.gen_aux})
       b->release();

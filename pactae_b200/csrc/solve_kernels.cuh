@@ -306,6 +306,79 @@ __global__ void k_invert_verify(const int32_t *__restrict__ pref_w, const int32_
 }
 
 // ---------------------------------------------------------------------------
+// Man-major copy of the rank matrix: rankT[m][w] = rank[w][m].  A solve's
+// proposals read "her rank of him" for every candidate a man scans; in the
+// woman-major matrix those reads fall in as many rows as candidates, in the
+// man-major one they stay in the man's own row, which stays in cache while
+// he scans.  Tiles of 64 x 64 go through shared memory so that both the
+// reads and the writes are coalesced; a persistent grid walks the tiles.
+// ---------------------------------------------------------------------------
+// uint16 with n even: every row starts 4-byte aligned, so pairs of elements
+// move as one 32-bit word and a warp reads or writes 128 bytes of a row.
+__global__ void __launch_bounds__(512) k_transpose_u16x2(const uint16_t *__restrict__ src, uint16_t *__restrict__ dst,
+                                                         int n, Control *ctrl, int gate) {
+  if (!gate_open(gate, ctrl)) return;
+  __shared__ uint16_t tile[64][66];
+  const int lane = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 16
+  const int tiles = (n + 63) / 64;
+  const long long total = static_cast<long long>(tiles) * tiles;
+  for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+    const int r0 = static_cast<int>(t / tiles) * 64, c0 = static_cast<int>(t % tiles) * 64;
+    const int c = c0 + 2 * lane;  // even, so c < n implies c + 1 < n
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int r = r0 + ty + 16 * k;
+      if (r < n && c < n) {
+        const uint32_t v = *reinterpret_cast<const uint32_t *>(src + static_cast<size_t>(r) * n + c);
+        tile[ty + 16 * k][2 * lane] = static_cast<uint16_t>(v & 0xFFFFu);
+        tile[ty + 16 * k][2 * lane + 1] = static_cast<uint16_t>(v >> 16);
+      }
+    }
+    __syncthreads();
+    const int oc = r0 + 2 * lane;  // output columns are source rows
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int orow = c0 + ty + 16 * k;  // output rows are source columns
+      if (orow < n && oc < n) {
+        const uint32_t v = static_cast<uint32_t>(tile[2 * lane][ty + 16 * k]) |
+                           (static_cast<uint32_t>(tile[2 * lane + 1][ty + 16 * k]) << 16);
+        *reinterpret_cast<uint32_t *>(dst + static_cast<size_t>(orow) * n + oc) = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(512) k_transpose(const T *__restrict__ src, T *__restrict__ dst, int n,
+                                                   Control *ctrl, int gate) {
+  if (!gate_open(gate, ctrl)) return;
+  __shared__ T tile[64][65];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 16
+  const int tiles = (n + 63) / 64;
+  const long long total = static_cast<long long>(tiles) * tiles;
+  for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+    const int r0 = static_cast<int>(t / tiles) * 64, c0 = static_cast<int>(t % tiles) * 64;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int r = r0 + ty + 16 * k, c = c0 + tx + 32 * j;
+        if (r < n && c < n) tile[ty + 16 * k][tx + 32 * j] = src[static_cast<size_t>(r) * n + c];
+      }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int r = c0 + ty + 16 * k, c = r0 + tx + 32 * j;  // dst row = src column
+        if (r < n && c < n) dst[static_cast<size_t>(r) * n + c] = tile[tx + 32 * j][ty + 16 * k];
+      }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Full validation (SMP_F_VALIDATE): every row of a preference matrix is a
 // permutation of 0..n-1.  One CTA per row at a time with an n-bit shared
 // bitmap.  Dynamic shared memory: ceil(n/32) * 4 bytes.
@@ -339,11 +412,12 @@ __global__ void __launch_bounds__(512) k_validate_rows(const int32_t *__restrict
 }
 
 // ---------------------------------------------------------------------------
-// Prefix gather (rank mode): prefix[m][r] = w << 16 | rank[w][m] for
-// w = pref_m[m][r], r < K.  An out-of-range woman is reported and her entry
+// Prefix gather (rank mode): prefix[m][r] = w << 16 | rankT[m][w] for
+// w = pref_m[m][r], r < K, from the man-major rank matrix (a man's entries
+// come from his own row).  An out-of-range woman is reported and her entry
 // set to 0xFFFFFFFF.
 // ---------------------------------------------------------------------------
-__global__ void k_prefix(const int32_t *__restrict__ pref_m, const uint16_t *__restrict__ rank,
+__global__ void k_prefix(const int32_t *__restrict__ pref_m, const uint16_t *__restrict__ rankT,
                          uint32_t *__restrict__ prefix, int n, int K, Control *ctrl, int gate) {
   if (!gate_open(gate, ctrl)) return;
   const size_t total = static_cast<size_t>(n) * K;
@@ -354,7 +428,7 @@ __global__ void k_prefix(const int32_t *__restrict__ pref_m, const uint16_t *__r
     const int w = __ldg(pref_m + static_cast<size_t>(m) * n + r);
     uint32_t e = 0xFFFFFFFFu;
     if (static_cast<unsigned>(w) < static_cast<unsigned>(n)) {
-      e = (static_cast<uint32_t>(w) << 16) | __ldg(rank + static_cast<size_t>(w) * n + m);
+      e = (static_cast<uint32_t>(w) << 16) | __ldg(rankT + static_cast<size_t>(m) * n + w);
     } else {
       report(ctrl, kStatusInvalidInput, w);
     }
@@ -482,7 +556,8 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
     if (lane == 0) free_now = ld_relaxed_s32(&ctrl->free_count);  // consumed after the window loads
     const int hold_m = m, hold_pos = pos;
     const auto keep_going = [&]() { return __shfl_sync(kFullMask, free_now, 0) > tail_threshold; };
-    const int rc = man_step<kMaxSub>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, ahead, settled,
+    const int rc = man_step<kMaxSub, true, true, 1, true>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m,
+                                                         pos, S, ahead, settled,
                                      hops, bad_value);
     if (rc == kStepMoved) continue;
     if (rc == kStepMatchedFree) {
@@ -631,7 +706,8 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
       }
       S = 1;
     }
-    const int rc = man_step<kMaxSub, (kMaxSub < 8), true, (kMaxSub == 8 ? 8 : 1)>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, ahead, settled,
+    const int rc = man_step<kMaxSub, (kMaxSub < 8), true, (kMaxSub == 8 ? 8 : 1), true>(
+        bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, ahead, settled,
                                      hops, bad_value);
     if (rc == kStepMoved || rc == kStepMatchedFree) continue;
     if (rc == kStepBad) {

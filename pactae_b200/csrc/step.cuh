@@ -31,7 +31,9 @@ __device__ __forceinline__ uint32_t issue_choice(const int32_t *__restrict__ pre
 
 // kLdg: the rank matrix is in global memory and read through the read-only
 // path; false when it may be in shared memory (the batch kernel).
-template <bool kLdg = true, typename RankT>
+// kManMajor: the matrix is stored man-major (rank[m][w] = her rank of him),
+// so a man's scan stays within his own row; else woman-major (rank[w][m]).
+template <bool kLdg = true, bool kManMajor = false, typename RankT>
 __device__ __forceinline__ int finish_choice(uint32_t raw, const RankT *__restrict__ rank, int K, int n, bool query,
                                              int m, int r, int &w, uint32_t &rk) {
   if (r >= n) return 3;
@@ -43,16 +45,17 @@ __device__ __forceinline__ int finish_choice(uint32_t raw, const RankT *__restri
   if (query) return 1;
   w = static_cast<int>(raw);
   if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) return 2;
-  const RankT *p = rank + static_cast<size_t>(w) * n + m;
+  const RankT *p = kManMajor ? rank + static_cast<size_t>(m) * n + w : rank + static_cast<size_t>(w) * n + m;
   rk = static_cast<uint32_t>(kLdg ? __ldg(p) : *p);
   return 0;
 }
 
-template <bool kLdg = true, typename RankT>
+template <bool kLdg = true, bool kManMajor = false, typename RankT>
 __device__ __forceinline__ int load_choice(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank,
                                            const uint32_t *__restrict__ prefix, int K, int n, bool query, int m,
                                            int r, int &w, uint32_t &rk) {
-  return finish_choice<kLdg>(issue_choice(pref_m, prefix, K, n, query, m, r), rank, K, n, query, m, r, w, rk);
+  return finish_choice<kLdg, kManMajor>(issue_choice(pref_m, prefix, K, n, query, m, r), rank, K, n, query, m, r, w,
+                                        rk);
 }
 
 // The window of the man a warp will carry next, loaded before it is known
@@ -183,8 +186,8 @@ __device__ __forceinline__ int try_window(const Bids &bids, int lane, int w, uin
 
 // kSReset: the look-ahead (in windows) a man starts with after a move; 1 for
 // chains that end within a few choices, kMaxSub where displaced men scan deep.
-template <int kMaxSub, bool kAhead = true, bool kLdg = true, int kSReset = 1, typename RankT, typename Bids,
-          typename Check>
+template <int kMaxSub, bool kAhead = true, bool kLdg = true, int kSReset = 1, bool kManMajor = false,
+          typename RankT, typename Bids, typename Check>
 __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, const int32_t *__restrict__ pref_m,
                                         const RankT *__restrict__ rank, const uint32_t *__restrict__ prefix, int K,
                                         int n, bool query, int lane, int &m, int &pos, int &S, Ahead &ahead,
@@ -197,7 +200,7 @@ __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, cons
     const uint32_t raw =
         (kAhead && ahead.m == m && ahead.pos == pos) ? ahead.raw : issue_choice(pref_m, prefix, K, n, query, m, r);
     if (kAhead) ahead.m = -1;
-    const int st0 = finish_choice<kLdg>(raw, rank, K, n, query, m, r, w0, rk0);
+    const int st0 = finish_choice<kLdg, kManMajor>(raw, rank, K, n, query, m, r, w0, rk0);
     typename Bids::Word cw = 0;
     uint32_t cr = 0u;
     if (st0 == 0) {
@@ -251,7 +254,7 @@ __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, cons
     if (s < S) {
       const int r = pos + 32 * s + lane;
       if (r < n) {
-        st[s] = load_choice<kLdg>(pref_m, rank, prefix, K, n, query, m, r, w[s], rk[s]);
+        st[s] = load_choice<kLdg, kManMajor>(pref_m, rank, prefix, K, n, query, m, r, w[s], rk[s]);
         if (st[s] == 0) cr[s] = bids.cur_rank(w[s]);
       }
     }
