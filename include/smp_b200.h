@@ -274,7 +274,7 @@ typedef struct smp_server_cfg {
   int32_t device;          /* CUDA device ordinal                                    */
   int32_t max_wave;        /* most requests one batched launch takes; 0 = 256        */
   int32_t route_n;         /* requests with n above this use the all-SM pipeline;    */
-                           /* 0 = 4096                                               */
+                           /* 0 = 1024                                               */
   int32_t waves;           /* batched launches in flight at once; 0 = 2              */
   uint64_t hbm_budget;     /* bytes of admitted requests' preference and rank        */
                            /* matrices (10 n^2 per request); 0 = 64 GiB              */

@@ -6,23 +6,49 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <array>
 #include <string>
 
 #include "smp_b200.h"
 
 namespace smpb200 {
 
-// Grow-only device allocation.
+// The library's memory pool on a device (smp_b200.cu): created on first use,
+// it keeps freed memory for later allocations until trim_device_pool.
+cudaMemPool_t device_pool(int device);
+void trim_device_pool(int device);
+
+// Grow-only device allocation.  Bound to a pool and a stream, it allocates
+// and frees in that stream's order (cudaMallocFromPoolAsync / cudaFreeAsync),
+// so growing a buffer waits for nothing else on the device; cudaFree would
+// wait for every stream.  Unbound, it uses cudaMalloc / cudaFree.
 struct DeviceBuf {
   void *ptr = nullptr;
   size_t bytes = 0;
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t stream = nullptr;
 
+  void bind(cudaMemPool_t p, cudaStream_t s) {
+    pool = p;
+    stream = s;
+  }
   int ensure(size_t need) {
     if (need <= bytes && ptr) return SMP_OK;
     release();
     if (need == 0) need = 16;
-    if (cudaMalloc(&ptr, need) != cudaSuccess) {
+    if (!allocate(need)) {
       cudaGetLastError();  // clear the sticky-free allocation error
+      if (pool) {
+        // Memory freed on other streams may still sit in the pool: wait for
+        // this stream, hand what is unused back and try once more.
+        cudaStreamSynchronize(stream);
+        cudaMemPoolTrimTo(pool, 0);
+        if (allocate(need)) {
+          bytes = need;
+          return SMP_OK;
+        }
+        cudaGetLastError();
+      }
       ptr = nullptr;
       bytes = 0;
       return SMP_ERR_OOM;
@@ -31,9 +57,18 @@ struct DeviceBuf {
     return SMP_OK;
   }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+      if (pool)
+        cudaFreeAsync(ptr, stream);
+      else
+        cudaFree(ptr);
+    }
     ptr = nullptr;
     bytes = 0;
+  }
+  bool allocate(size_t need) {
+    if (pool) return cudaMallocFromPoolAsync(&ptr, need, pool, stream) == cudaSuccess;
+    return cudaMalloc(&ptr, need) == cudaSuccess;
   }
   template <typename T>
   T *as() const { return static_cast<T *>(ptr); }
@@ -94,6 +129,11 @@ struct Ctx {
   static constexpr int kCopyChunks = 16;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_chunk[kCopyChunks] = {};
+  std::array<DeviceBuf *, 19> buffers() {
+    return {&d_pref_m, &d_pref_w, &d_rank,    &d_rankT,    &d_prefix, &d_bid,    &d_tailq,
+            &d_seen,   &d_ctrl,   &d_match,   &d_husband,  &d_prank,  &d_qcnt,   &d_qlist,
+            &gen_keys_a, &gen_keys_b, &gen_seg, &gen_temp, &gen_aux};
+  }
   int launches = 0;  // kernels launched since the last stage / call
   smp_stats stats = {};
 
@@ -121,6 +161,7 @@ struct Ctx {
 int solve_enqueue(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
                   uint32_t flags);
 int solve_finish(Ctx &c, uint32_t flags, smp_stats *st);
+int reserve_buffers(Ctx &c, int32_t n);
 
 // batch.cu: the batch kernel on a caller's stream and table (serving loop).
 struct BatchInstance;

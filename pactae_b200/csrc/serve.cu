@@ -88,6 +88,7 @@ struct smp_server {
   std::deque<Request *> pending, small_q, large_q;
   std::vector<Wave> waves;
   uint64_t used = 0;
+  cudaMemPool_t pool = nullptr;  // device_pool of the server's device
   int grid = 0;
   size_t slab_elems = 0;
 };
@@ -111,9 +112,11 @@ void finish(smp_server &s, Request *r, int status, int64_t proposals) {
 
 // Host-pointer requests: device copies of the lists (and the output) on the
 // given stream.  Returns the status.
-int stage_request(Request *r, cudaStream_t st) {
+int stage_request(Request *r, cudaStream_t st, cudaMemPool_t pool) {
   if (r->flags & SMP_F_DEVICE_PTRS) return SMP_OK;
   const size_t bytes = sizeof(int32_t) * static_cast<size_t>(r->n) * r->n;
+  // allocated and freed in the order of the stream that runs the request
+  for (DeviceBuf *b : {&r->d_pm, &r->d_pw, &r->d_match}) b->bind(pool, st);
   if (r->d_pm.ensure(bytes) || r->d_pw.ensure(bytes) || r->d_match.ensure(sizeof(int32_t) * r->n))
     return SMP_ERR_OOM;
   if (cudaMemcpyAsync(r->d_pm.ptr, r->pm, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -148,7 +151,7 @@ void launch_wave(smp_server &s, Wave &w) {
   for (int i = 0; i < count && !rc; ++i) {
     Request *r = w.reqs[i];
     r->t_launch = now;
-    rc = stage_request(r, w.stream);
+    rc = stage_request(r, w.stream, s.pool);
     w.h_table[i] = smp_instance{r->dev_pm(), r->dev_pw(), r->dev_match(), r->n, SMP_ERR_NOT_READY, 0};
   }
   if (!rc && (cudaMemcpyAsync(w.table.ptr, w.h_table, sizeof(smp_instance) * count, cudaMemcpyHostToDevice,
@@ -194,7 +197,7 @@ void launch_large(smp_server &s, smp_server::LargeSlot &slot) {
   s.large_q.pop_front();
   Ctx &lc = slot.ctx->c;
   r->t_launch = Clock::now();
-  int rc = stage_request(r, lc.stream);
+  int rc = stage_request(r, lc.stream, s.pool);
   if (!rc) rc = solve_enqueue(lc, r->dev_pm(), r->dev_pw(), r->n, r->dev_match(), SMP_F_DEVICE_PTRS);
   if (!rc) rc = unstage_request(r, lc.stream);
   if (!rc && cudaEventRecord(slot.done, lc.stream) != cudaSuccess) rc = lc.fail_cuda("large event");
@@ -281,7 +284,7 @@ void destroy_server(smp_server *s) {
     if (slot.done) cudaEventDestroy(slot.done);
     if (slot.ctx) smp_b200_destroy(slot.ctx);
   }
-  if (s->ctx) smp_b200_destroy(s->ctx);
+  if (s->ctx) smp_b200_destroy(s->ctx);  // also trims the device pool
   for (auto &kv : s->tickets) delete kv.second;
   delete s;
 }
@@ -296,7 +299,7 @@ int smp_b200_server_create(const smp_server_cfg *cfg, smp_server **out) {
   auto *s = new (std::nothrow) smp_server();
   if (!s) return SMP_ERR_OOM;
   if (cfg) s->cfg = *cfg;
-  if (s->cfg.route_n <= 0) s->cfg.route_n = 4096;
+  if (s->cfg.route_n <= 0) s->cfg.route_n = 1024;
   s->cfg.route_n = std::min(s->cfg.route_n, SMP_B200_BATCH_MAX_N);
   if (s->cfg.waves <= 0) s->cfg.waves = 2;
   if (s->cfg.hbm_budget == 0) s->cfg.hbm_budget = 64ull << 30;
@@ -312,6 +315,7 @@ int smp_b200_server_create(const smp_server_cfg *cfg, smp_server **out) {
   }
   Ctx &c = s->ctx->c;
   DeviceGuard g(c.device);
+  s->pool = device_pool(c.device);
   const int max_wave = s->cfg.max_wave > 0 ? s->cfg.max_wave : 256;
   const int per_sm = s->cfg.ctas_per_sm > 0 ? s->cfg.ctas_per_sm : 2;
   s->grid = std::max(1, std::min(max_wave, c.sm_count * per_sm));
@@ -331,6 +335,14 @@ int smp_b200_server_create(const smp_server_cfg *cfg, smp_server **out) {
   }
   for (auto &slot : s->large)
     if (!rc && cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming) != cudaSuccess) rc = SMP_ERR_CUDA;
+  // Each large slot holds the buffers of the largest request the budget
+  // admits from the start: growing them while others run would stall the
+  // burst that brought the first large requests.
+  int reserve_n = SMP_B200_BATCH_MAX_N;
+  while (reserve_n > s->cfg.route_n && 10ull * reserve_n * reserve_n > s->cfg.hbm_budget) reserve_n /= 2;
+  if (reserve_n > s->cfg.route_n)
+    for (auto &slot : s->large)
+      if (!rc) rc = reserve_buffers(slot.ctx->c, reserve_n);
   if (rc) {
     cudaGetLastError();
     destroy_server(s);

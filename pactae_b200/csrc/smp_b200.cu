@@ -4,6 +4,7 @@
 // solve_kernels.cuh and generate.cu.
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <type_traits>
 
 #include "common.cuh"
@@ -513,6 +514,60 @@ void fill_stats(Ctx &c, bool timed_phases) {
 
 namespace smpb200 {
 
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+}  // namespace
+
+cudaMemPool_t device_pool(int device) {
+  if (device < 0 || device >= kMaxDevices) return nullptr;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pools[device]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;  // buffers then fall back to cudaMalloc
+    }
+    // Keep freed memory for the next allocation instead of returning it at
+    // every synchronisation.
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pools[device] = pool;
+  }
+  return g_pools[device];
+}
+
+void trim_device_pool(int device) {
+  if (device < 0 || device >= kMaxDevices) return;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (g_pools[device]) cudaMemPoolTrimTo(g_pools[device], 0);
+}
+
+// Allocates every buffer a device-pointer solve of size n uses, in either
+// mode and with the checker, so that later solves up to n allocate nothing.
+int reserve_buffers(Ctx &c, int32_t n) {
+  if (n <= 0 || n > SMP_B200_MAX_N) return SMP_ERR_INVALID_ARG;
+  stage_reset(c, n);
+  const size_t nn = static_cast<size_t>(n) * n;
+  int rc = c.d_ctrl.ensure(sizeof(Control));
+  if (!rc) rc = c.d_seen.ensure(((static_cast<size_t>(n) + 31) / 32) * 4);
+  if (!rc) rc = init_buffers(c);
+  if (!rc) rc = c.d_rankT.ensure(nn * c.rank_bytes);
+  if (!rc && c.query_ok) rc = c.d_qcnt.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (!rc && c.query_ok)
+    rc = c.d_qlist.ensure(sizeof(uint32_t) * static_cast<size_t>(n) * query_capacity(n, c.K));
+  if (!rc) rc = c.d_husband.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (!rc) rc = c.d_prank.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (!rc) rc = c.sync("reserve");
+  c.n = 0;
+  return rc;
+}
+
 // Enqueues a whole solve on c.stream with no host round trip (stage,
 // precheck, init, core, post, the match copy, optional check, control
 // readback).  The caller synchronises the stream, then calls solve_finish.
@@ -724,6 +779,8 @@ int smp_b200_create(smp_ctx **out, const smp_cfg *cfg) {
     delete ctx;
     return SMP_ERR_CUDA;
   }
+  if (cudaMemPool_t pool = device_pool(c.device))
+    for (DeviceBuf *b : c.buffers()) b->bind(pool, c.stream);
   for (auto &e : c.ev) {
     if (cudaEventCreate(&e) != cudaSuccess) {
       smp_b200_destroy(ctx);
@@ -745,12 +802,11 @@ void smp_b200_destroy(smp_ctx *ctx) {
   Ctx &c = ctx->c;
   {
     DeviceGuard g(c.device);
-    if (c.stream) cudaStreamSynchronize(c.stream);
-    for (DeviceBuf *b : {&c.d_pref_m, &c.d_pref_w, &c.d_rank, &c.d_rankT, &c.d_prefix, &c.d_bid, &c.d_tailq, &c.d_seen,
-                         &c.d_ctrl, &c.d_match, &c.d_husband, &c.d_prank, &c.d_qcnt, &c.d_qlist,
-                         &c.gen_keys_a, &c.gen_keys_b, &c.gen_seg, &c.gen_temp, &c.gen_aux})
-      b->release();
     if (c.copy_stream) cudaStreamSynchronize(c.copy_stream);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    for (DeviceBuf *b : c.buffers()) b->release();
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    trim_device_pool(c.device);
     for (auto &e : c.ev)
       if (e) cudaEventDestroy(e);
     for (auto &e : c.ev_chunk)
