@@ -232,21 +232,25 @@ int enqueue_query_index(Ctx &c) {
 }
 
 int enqueue_qinvert(Ctx &c, int w0, int w1) {
+  // n <= kColorMaxN: the pipelined kernel with colour-tagged slots;
+  // larger n: the one with a clearing pass per row.
+  const auto kernel = c.n <= kColorMaxN ? k_qinvert_c : k_qinvert;
   const size_t smem = row_smem_bytes<uint16_t>(c.n);
-  if (cudaFuncSetAttribute(k_qinvert, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
       cudaSuccess)
     return c.fail_cuda("k_qinvert smem attribute");
+  const int block = c.n <= kColorMaxN ? 256 : 512;
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_qinvert, 512, smem) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess) {
     cudaGetLastError();
     per_sm = 1;
   }
   const int qgrid = std::max(1, std::min(w1 - w0, c.sm_count * std::max(per_sm, 1)));
-  k_qinvert<<<qgrid, 512, smem, c.stream>>>(c.pref_w, c.n, c.K, query_capacity(c.n, c.K), c.d_qcnt.as<int32_t>(),
-                                            c.d_qlist.as<uint32_t>(),
-                                            c.d_prefix.as<uint32_t>(), c.d_ctrl.as<Control>(), w0, w1);
+  kernel<<<qgrid, block, smem, c.stream>>>(c.pref_w, c.n, c.K, query_capacity(c.n, c.K), c.d_qcnt.as<int32_t>(),
+                                         c.d_qlist.as<uint32_t>(), c.d_prefix.as<uint32_t>(), c.d_ctrl.as<Control>(),
+                                         w0, w1);
   c.launches++;
-  return c.check_launch("k_qinvert");
+  return c.check_launch(c.n <= kColorMaxN ? "k_qinvert_c" : "k_qinvert");
 }
 
 int enqueue_query(Ctx &c) {

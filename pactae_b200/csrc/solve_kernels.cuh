@@ -509,6 +509,133 @@ __global__ void __launch_bounds__(512) k_qinvert(const int32_t *__restrict__ pre
   if (bad) report(ctrl, kStatusInvalidInput, -1);
 }
 
+// Rows [w0, w1) for n <= kColorMaxN, written to keep pref_w streaming while a
+// row is checked and answered.  Each CTA handles rows w0 + blockIdx.x + k *
+// gridDim.x; the k-th row's slots are written as rank | (k & 1) << 15, so a
+// slot this row did not write still carries the other colour (the row before
+// it, or the fill at the start) and validation needs no clearing pass.  The
+// next row's first batch of 16-byte loads is issued before the current row
+// is validated and answered.  One barrier ends the scatter, one the answers.
+// After a row that is not a permutation the colours may no longer tell, but
+// that row has already reported the error.
+constexpr int kColorMaxN = 32767;
+
+struct RowSpan {
+  const int32_t *row;  // first element
+  const int4 *rq;      // first 16-byte aligned element (row + head)
+  int head;            // scalars before rq (0..3)
+  int nq;              // 16-byte chunks
+  int tail;            // scalars after them (0..3)
+};
+
+__device__ __forceinline__ RowSpan row_span(const int32_t *pref_w, int w, int n) {
+  RowSpan s;
+  s.row = pref_w + static_cast<size_t>(w) * n;
+  s.head = min(n, static_cast<int>(((16u - (reinterpret_cast<uintptr_t>(s.row) & 15u)) & 15u) >> 2));
+  s.rq = reinterpret_cast<const int4 *>(s.row + s.head);
+  s.nq = (n - s.head) >> 2;
+  s.tail = n - s.head - 4 * s.nq;
+  return s;
+}
+
+// Batch starting at chunk `base`: chunk base + tid + j * nthr into v[j].
+__device__ __forceinline__ void row_batch_load(const RowSpan &s, int base, int4 (&v)[4]) {
+  const int nthr = blockDim.x;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int i = base + static_cast<int>(threadIdx.x) + j * nthr;
+    v[j] = i < s.nq ? __ldcs(s.rq + i) : make_int4(0, 0, 0, 0);
+  }
+}
+
+__device__ __forceinline__ void scatter_c(uint16_t *srow, int m, int r, uint32_t cbit, int n, bool &bad) {
+  if (static_cast<unsigned>(m) < static_cast<unsigned>(n)) {
+    srow[m] = static_cast<uint16_t>(static_cast<uint32_t>(r) | cbit);
+  } else {
+    bad = true;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_qinvert_c(const int32_t *__restrict__ pref_w, int n, int K, int qcap,
+                                                      const int32_t *__restrict__ qcnt,
+                                                      const uint32_t *__restrict__ qlist,
+                                                      uint32_t *__restrict__ prefix, Control *ctrl, int w0, int w1) {
+  if (!gate_open(kGateModeQuery, ctrl) || ld_volatile_s32(&ctrl->retry)) return;
+  int w = w0 + static_cast<int>(blockIdx.x);
+  if (w >= w1) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint16_t *srow = reinterpret_cast<uint16_t *>(smem_raw);
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;
+  const int chunks = (n + 7) / 8;
+  uint4 *s4 = reinterpret_cast<uint4 *>(srow);
+  // colour 1 everywhere: the first row (colour 0) must write every slot
+  for (int c = tid; c < chunks; c += nthr) s4[c] = make_uint4(~0u, ~0u, ~0u, ~0u);
+  bool bad = false;
+  RowSpan s = row_span(pref_w, w, n);
+  int4 a[4];
+  row_batch_load(s, 0, a);
+  int edge_head = tid < s.head ? __ldcs(s.row + tid) : 0;
+  int edge_tail = tid < s.tail ? __ldcs(s.row + s.head + 4 * s.nq + tid) : 0;
+  __syncthreads();  // the fill before the first scatter
+  for (int k = 0;; ++k) {
+    const uint32_t cbit = static_cast<uint32_t>(k & 1) << 15;
+    if (tid < s.head) scatter_c(srow, edge_head, tid, cbit, n, bad);
+    if (tid < s.tail) scatter_c(srow, edge_tail, s.head + 4 * s.nq + tid, cbit, n, bad);
+    for (int base = 0; base < s.nq; base += 4 * nthr) {
+      if (base > 0) row_batch_load(s, base, a);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int i = base + tid + j * nthr;
+        if (i < s.nq) {
+          const int r = s.head + 4 * i;
+          scatter_c(srow, a[j].x, r, cbit, n, bad);
+          scatter_c(srow, a[j].y, r + 1, cbit, n, bad);
+          scatter_c(srow, a[j].z, r + 2, cbit, n, bad);
+          scatter_c(srow, a[j].w, r + 3, cbit, n, bad);
+        }
+      }
+    }
+    __syncthreads();  // row w complete in shared memory
+    const int wn = w + static_cast<int>(gridDim.x);
+    const RowSpan sn = row_span(pref_w, wn < w1 ? wn : w, n);
+    if (wn < w1) {
+      row_batch_load(sn, 0, a);
+      edge_head = tid < sn.head ? __ldcs(sn.row + tid) : 0;
+      edge_tail = tid < sn.tail ? __ldcs(sn.row + sn.head + 4 * sn.nq + tid) : 0;
+    }
+    // validation: every slot carries this row's colour
+    const uint32_t want = cbit ? 0x80008000u : 0u;
+    for (int c = tid; c < chunks; c += nthr) {
+      const uint4 v = s4[c];
+      const int tailn = n - c * 8;
+      uint32_t m0 = 0x80008000u, m1 = 0x80008000u, m2 = 0x80008000u, m3 = 0x80008000u;
+      if (tailn < 8) {  // halves past n keep the fill; leave them out
+        const auto keep = [tailn](int half) -> uint32_t {
+          return (half < tailn ? 0x00008000u : 0u) | (half + 1 < tailn ? 0x80000000u : 0u);
+        };
+        m0 = keep(0);
+        m1 = keep(2);
+        m2 = keep(4);
+        m3 = keep(6);
+      }
+      bad |= (((v.x ^ want) & m0) | ((v.y ^ want) & m1) | ((v.z ^ want) & m2) | ((v.w ^ want) & m3)) != 0u;
+    }
+    const uint32_t *bucket = qlist + static_cast<size_t>(w) * qcap;
+    const int count = min(__ldg(qcnt + w), qcap);
+    for (int q = tid; q < count; q += nthr) {
+      const uint32_t e = bucket[q];
+      const uint32_t m = e >> 16, r = e & 0xFFFFu;
+      prefix[static_cast<size_t>(m) * K + r] = (static_cast<uint32_t>(w) << 16) | (srow[m] & 0x7FFFu);
+    }
+    __syncthreads();  // answers read before the next row overwrites
+    if (wn >= w1) break;
+    w = wn;
+    s = sn;
+  }
+  if (bad) report(ctrl, kStatusInvalidInput, -1);
+}
+
 // ---------------------------------------------------------------------------
 // Bulk proposals on every SM.  Each warp carries one free man at a time
 // (man_step above, 64-bit bids in HBM).  A man accepted by a free woman

@@ -213,6 +213,32 @@ def test_invalid_inputs_rejected(ctx):
     assert np.array_equal(match, oracle.gs_seq(pm, pw)[0])
 
 
+@pytest.mark.parametrize("n,row", [(4999, 10), (4999, 4990), (6000, 3001)])
+@pytest.mark.parametrize("defect", ["duplicate", "out_of_range"])
+@pytest.mark.parametrize("host", [False, True])
+def test_bad_row_deep_in_the_inversion(ctx, n, row, defect, host):
+    # At these sizes each CTA of the query-mode inversion works through many
+    # rows, so a bad row is found after rows that were permutations (row 10
+    # is the first row of its CTA).  Host inputs take the streamed path.
+    pm, pw = ctx.generate(pb.SMP_GEN_UNIFORM, n, seed=77)
+    pw = pw.clone()
+    if defect == "duplicate":
+        pw[row, 5] = pw[row, 6]
+    else:
+        pw[row, n - 1] = n + 5
+    if host:
+        pm, pw = to_host(pm), to_host(pw)
+    with pytest.raises(pb.SmpError) as e:
+        ctx.solve(pm, pw)
+    assert e.value.status == pb.SMP_ERR_INVALID_INPUT
+    # the same context solves the intact instance afterwards
+    pm2, pw2 = ctx.generate(pb.SMP_GEN_UNIFORM, n, seed=77)
+    match, st = ctx.solve(pm2, pw2)
+    if n == 4999 and row == 10 and defect == "duplicate" and not host:
+        want, props = oracle.gs_seq(to_host(pm2), to_host(pw2))
+        assert np.array_equal(to_host(match), want) and st["proposals"] == props
+
+
 def test_bad_arguments(ctx):
     with pytest.raises(pb.SmpError) as e:
         ctx.generate(pb.SMP_GEN_SOLO, 2, seed=1)
