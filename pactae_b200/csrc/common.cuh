@@ -35,7 +35,9 @@ struct Control {
   int32_t allow_query;    // host switch: 1 if the query mode may be chosen
   int32_t blocks_done;    // precheck: blocks that finished (the last one decides)
   int32_t distinct;       // precheck: number of distinct first choices
-  int32_t pad0[3];
+  int32_t distinct_w;     // k_wdistinct: distinct first choices of the women
+  int32_t use_filter;     // k_wdistinct: k_bulk runs with its shared partner-rank filter
+  int32_t pad0;
   unsigned long long proposals;        // sum over men of (final position + 1)
   unsigned long long blocking;         // checker: blocking pairs
   unsigned long long check_proposals;  // checker: proposals recounted from the matching
@@ -43,6 +45,11 @@ struct Control {
   unsigned long long tail_proposals;   // proposals settled by k_tail
   unsigned int bulk_hops;              // accepted proposals in k_bulk
   unsigned int tail_hops;              // accepted proposals in k_tail
+  // Chains k_tail handed to k_tail_coop (man, next position), at most one
+  // per warp of the tail CTA; coop_count is 0 when none are waiting.
+  int32_t coop_count;
+  int32_t pad1;
+  int2 coop_chain[32];
 };
 
 __device__ __forceinline__ void report(Control *ctrl, int status, int value) {

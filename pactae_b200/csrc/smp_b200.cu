@@ -25,6 +25,9 @@ int query_capacity(int n, int K) { return std::min(n, K + K / 2 + 32); }
 // Host-pointer solves of at least this n stream their inputs (solve_streamed).
 constexpr int kStreamMinN = 4096;
 constexpr int kRankTailWindow = 256;
+// Chains left when k_tail hands the rest to k_tail_coop (one at a time, the
+// whole CTA scanning each).
+constexpr int kCoopChains = 4;
 constexpr int kU16MaxN = 65535;
 
 inline bool valid_ctx(const smp_ctx *ctx) { return ctx != nullptr && ctx->c.stream != nullptr; }
@@ -291,9 +294,33 @@ template <typename RankT, int kSub>
 int launch_bulk(Ctx &c, int round) {
   const RankT *rank = reinterpret_cast<const RankT *>(c.d_rankT.ptr);  // man-major
   const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
+  const int rank_threshold = c.tail_threshold > 0 ? std::min(c.tail_threshold, c.tail_threshold_rank) : 0;
+  const size_t filter = sizeof(uint32_t) * static_cast<size_t>(c.n);
+  if (round == 0 && filter + 1024 <= c.smem_optin) {  // the shared partner-rank filter fits
+    // k_wdistinct decides on the device which of the two variants runs
+    k_wdistinct<<<1, 1024, sizeof(uint32_t) * ((c.n + 31) / 32), c.stream>>>(c.pref_w, c.n, c.d_ctrl.as<Control>());
+    c.launches++;
+    int rc = c.check_launch("k_wdistinct");
+    if (rc) return rc;
+    const auto kernel = k_bulk<RankT, kSub, true>;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(filter)) !=
+        cudaSuccess)
+      return c.fail_cuda("k_bulk smem attribute");
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kFilterBlock, filter) != cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    kernel<<<c.sm_count * std::max(per_sm, 1), kFilterBlock, filter, c.stream>>>(
+        c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(), c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
+        c.n, c.tail_threshold, rank_threshold, round);
+    c.launches++;
+    rc = c.check_launch("k_bulk (filtered)");
+    if (rc) return rc;
+  }
   k_bulk<RankT, kSub><<<resident_grid(c, k_bulk<RankT, kSub>, 256), 256, 0, c.stream>>>(
       c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(), c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
-      c.n, c.tail_threshold, c.tail_threshold > 0 ? std::min(c.tail_threshold, c.tail_threshold_rank) : 0, round);
+      c.n, c.tail_threshold, rank_threshold, round);
   c.launches++;
   return c.check_launch("k_bulk");
 }
@@ -308,9 +335,18 @@ int launch_tail(Ctx &c, int round, int only_mode) {
     return c.fail_cuda("k_tail smem attribute");
   k_tail<RankT, kSub><<<1, 1024, smem, c.stream>>>(c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(),
                                                    c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
-                                                   c.d_match.as<int32_t>(), c.n, round, only_mode);
+                                                   c.d_match.as<int32_t>(), c.n, round, only_mode, kCoopChains);
   c.launches++;
-  return c.check_launch("k_tail");
+  int rc = c.check_launch("k_tail");
+  if (rc) return rc;
+  // the last chains, if k_tail handed them over
+  if (cudaFuncSetAttribute(k_tail_coop<RankT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess)
+    return c.fail_cuda("k_tail_coop smem attribute");
+  k_tail_coop<RankT><<<1, 1024, smem, c.stream>>>(c.pref_m, rank, c.d_bid.as<unsigned long long>(),
+                                                  c.d_ctrl.as<Control>(), c.d_match.as<int32_t>(), c.n);
+  c.launches++;
+  return c.check_launch("k_tail_coop");
 }
 
 int launch_tail_query(Ctx &c) {

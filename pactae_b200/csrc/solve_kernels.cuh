@@ -29,6 +29,8 @@
 // run: no host round trip inside a solve.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "step.cuh"
 
@@ -647,13 +649,71 @@ __global__ void __launch_bounds__(256) k_qinvert_c(const int32_t *__restrict__ p
 // rank-mode retry round.
 // round 0: gate Main; round 1: gate Retry (rank mode).
 // ---------------------------------------------------------------------------
-template <typename RankT, int kMaxSub>
-__global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank,
-                                              const uint32_t *__restrict__ prefix, int K,
-                                              unsigned long long *bid, Control *ctrl, int2 *tail_queue, int n,
-                                              int tail_threshold_query, int tail_threshold_rank, int round) {
-  if (!gate_open(round == 0 ? kGateMain : kGateRetry, ctrl)) return;
-  if (round == 0 && ld_volatile_s32(&ctrl->retry)) return;  // a query bucket overflowed
+// kFilter: bids go through FilteredBids, a per-CTA bound on each woman's
+// partner rank in 4 n bytes of shared memory (one CTA of kFilterBlock threads
+// per SM); else GlobalBids.  Both variants are enqueued and the device runs
+// the one k_wdistinct chose (ctrl->use_filter).
+constexpr int kFilterBlock = 768;
+constexpr int kFilterMaxDistinct = 16;
+
+// ---------------------------------------------------------------------------
+// Chooses the bulk variant of a rank-mode round 0.  The filter pays off when
+// the men's lists are nearly all alike (at most kFilterMaxDistinct distinct
+// first choices: every man scans the same women) and the women's are not (at
+// least n / 4 distinct first choices: most of those proposals are rejections
+// by women who already hold a better man).  Where the women's lists are alike
+// too, most proposals displace someone and the filter only adds work.  One
+// CTA counts the women's distinct first choices in a shared bitmap.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_wdistinct(const int32_t *__restrict__ pref_w, int n, Control *ctrl) {
+  extern __shared__ uint32_t seen[];
+  if (!gate_open(kGateModeRank, ctrl) || ld_volatile_s32(&ctrl->distinct) > kFilterMaxDistinct) return;
+  const int words = (n + 31) >> 5;
+  for (int i = threadIdx.x; i < words; i += blockDim.x) seen[i] = 0u;
+  __syncthreads();
+  for (int w = threadIdx.x; w < n; w += blockDim.x) {
+    const int m = __ldg(pref_w + static_cast<size_t>(w) * n);
+    if (static_cast<unsigned>(m) < static_cast<unsigned>(n)) atomicOr(seen + (m >> 5), 1u << (m & 31));
+  }
+  __syncthreads();
+  __shared__ int s_count;
+  if (threadIdx.x == 0) s_count = 0;
+  __syncthreads();
+  int count = 0;
+  for (int i = threadIdx.x; i < words; i += blockDim.x) count += __popc(seen[i]);
+  atomicAdd(&s_count, count);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ctrl->distinct_w = s_count;
+    ctrl->use_filter = 4ll * s_count >= n ? 1 : 0;
+  }
+}
+
+template <typename RankT, int kMaxSub, bool kFilter = false>
+__global__ void __launch_bounds__(kFilter ? kFilterBlock : 256)
+    k_bulk(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank, const uint32_t *__restrict__ prefix,
+           int K, unsigned long long *bid, Control *ctrl, int2 *tail_queue, int n, int tail_threshold_query,
+           int tail_threshold_rank, int round) {
+  using Bids = typename std::conditional<kFilter, FilteredBids, GlobalBids>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t *lrank = reinterpret_cast<uint32_t *>(smem_raw);
+  if (kFilter) {
+    // The gates are read once for the CTA: the retry flag may be raised by
+    // another CTA while this one starts, and every thread must reach the
+    // barrier.
+    __shared__ int s_go;
+    if (threadIdx.x == 0)
+      s_go = round == 0 && ld_volatile_s32(&ctrl->use_filter) && gate_open(kGateMain, ctrl) &&
+             !ld_volatile_s32(&ctrl->retry);
+    __syncthreads();
+    if (!s_go) return;
+    for (int w = threadIdx.x; w < n; w += blockDim.x) lrank[w] = 0xFFFFFFFFu;
+    __syncthreads();
+  } else {
+    if (!gate_open(round == 0 ? kGateMain : kGateRetry, ctrl)) return;
+    if (round == 0 && ld_volatile_s32(&ctrl->retry)) return;  // a query bucket overflowed
+    if (round == 0 && ld_volatile_s32(&ctrl->use_filter)) return;  // the filtered variant runs
+  }
   const bool query = round == 0 && ld_volatile_s32(&ctrl->mode) == kModeQuery;
   // Free women left when the men move to the one-CTA tail: rank-mode
   // instances scan deep, which many SMs do faster, so they hand over later.
@@ -664,7 +724,9 @@ __global__ void __launch_bounds__(256) k_bulk(const int32_t *__restrict__ pref_m
   // the solve -- this kernel and the one-SM tail -- is a chain of dependent
   // reads of it, so each miss would cost a DRAM round trip on the chain.
   if (prefix != nullptr) prefetch_l2(prefix, static_cast<size_t>(n) * K * sizeof(uint32_t));
-  const GlobalBids bids{bid};
+  Bids bids;
+  bids.bid = bid;
+  if constexpr (kFilter) bids.lrank = lrank;
   int m = -1, pos = 0, S = 1, bad_value = 0;
   Ahead ahead;
   unsigned long long settled = 0;  // proposals this warp decided (lane 0's copy is used)
@@ -733,6 +795,26 @@ __device__ __forceinline__ void tail_setup(const unsigned long long *__restrict_
   }
 }
 
+// The tail's shared state into the bid buffer (4 n bytes of words, then 2 n
+// bytes of positions; the buffer holds 8 n) and back.
+__device__ __forceinline__ void coop_store(const uint32_t *sbid, const uint16_t *spos, unsigned long long *bid,
+                                           int n) {
+  uint32_t *gb = reinterpret_cast<uint32_t *>(bid);
+  uint16_t *gp = reinterpret_cast<uint16_t *>(gb + n);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    gb[i] = sbid[i];
+    gp[i] = spos[i];
+  }
+}
+__device__ __forceinline__ void coop_load(const unsigned long long *bid, uint32_t *sbid, uint16_t *spos, int n) {
+  const uint32_t *gb = reinterpret_cast<const uint32_t *>(bid);
+  const uint16_t *gp = reinterpret_cast<const uint16_t *>(gb + n);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    sbid[i] = gb[i];
+    spos[i] = gp[i];
+  }
+}
+
 // match[] and the proposal count (sum of final positions + 1) from the
 // shared state, after every chain has ended.  Called by the whole CTA.
 __device__ __forceinline__ void tail_finish(const uint32_t *sbid, const uint16_t *spos, int32_t *__restrict__ match,
@@ -778,10 +860,10 @@ template <typename RankT, int kMaxSub>
 __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pref_m,
                                                   const RankT *__restrict__ rank,
                                                   const uint32_t *__restrict__ prefix, int K,
-                                                  const unsigned long long *__restrict__ bid, Control *ctrl,
+                                                  unsigned long long *bid, Control *ctrl,
                                                   const int2 *__restrict__ tail_queue,
                                                   int32_t *__restrict__ match, int n, int round,
-                                                  int only_mode) {
+                                                  int only_mode, int coop_chains) {
   if (only_mode >= 0 && round == 0 && ld_volatile_s32(&ctrl->mode) != only_mode) return;
   if (round == 0 && ld_volatile_s32(&ctrl->perfect)) {
     write_perfect(pref_m, match, n, ctrl);
@@ -795,6 +877,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
   uint16_t *spos = reinterpret_cast<uint16_t *>(smem_raw + static_cast<size_t>(n) * 4);
   __shared__ int s_next;
   __shared__ int s_abort;
+  __shared__ int s_busy;  // warps carrying a chain
   __shared__ unsigned long long s_props;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -806,6 +889,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
   if (tid == 0) {
     s_next = 0;
     s_abort = 0;
+    s_busy = 0;
     s_props = 0;
     ctrl->tail_men = total;
   }
@@ -832,10 +916,28 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
         pos = 0;
       }
       S = 1;
+      if (lane == 0) atomicAdd(&s_busy, 1);
+    } else if (coop_chains > 0) {
+      // Once no man waits and only a few chains are left, each goes to
+      // k_tail_coop, which runs them one after another with the whole CTA
+      // scanning (Gale-Shapley's result does not depend on the order).
+      int hand = 0;
+      if (lane == 0)
+        hand = *reinterpret_cast<volatile int *>(&s_next) >= total &&
+               *reinterpret_cast<volatile int *>(&s_busy) <= coop_chains;
+      if (__shfl_sync(kFullMask, hand, 0)) {
+        if (lane == 0) {
+          const int e = atomicAdd(&ctrl->coop_count, 1);  // < 32: each warp hands over once
+          ctrl->coop_chain[e] = make_int2(m, pos);
+          atomicSub(&s_busy, 1);
+        }
+        break;
+      }
     }
     const int rc = man_step<kMaxSub, (kMaxSub < 8), true, (kMaxSub == 8 ? 8 : 1), true>(
         bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, ahead, settled,
                                      hops, bad_value);
+    if (rc == kStepMatchedFree && lane == 0) atomicSub(&s_busy, 1);
     if (rc == kStepMoved || rc == kStepMatchedFree) continue;
     if (rc == kStepBad) {
       if (lane == 0) report(ctrl, kStatusInvalidInput, bad_value);
@@ -851,6 +953,132 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
   }
   __syncthreads();
   if (s_abort || ld_volatile_s32(&ctrl->status)) return;
+  if (ld_volatile_s32(&ctrl->coop_count) > 0) {
+    // chains handed over: the shared state goes to k_tail_coop through the
+    // bid buffer, which this kernel no longer reads
+    coop_store(sbid, spos, bid, n);
+    return;
+  }
+  tail_finish(sbid, spos, match, n, ctrl, &s_props);
+}
+
+// ---------------------------------------------------------------------------
+// The chains k_tail handed over, one after another, each scanned by the
+// whole CTA: 1024 threads test up to 8 choices each per step (widening from
+// one while no candidate turns up), a CTA minimum picks the first woman who
+// would accept him, and one thread records the proposal.  With one chain
+// running nothing else changes a bid, so the first candidate always accepts
+// and no atomic is needed.  Deep chains (correlated and congested lists, where
+// a displaced man rejects hundreds of women before the next acceptance) move
+// up to 8192 choices per round trip instead of one warp's 256.  Then the CTA
+// writes match[] and the proposal count as k_tail would have.
+// ---------------------------------------------------------------------------
+template <typename RankT>
+__global__ void __launch_bounds__(1024, 1) k_tail_coop(const int32_t *__restrict__ pref_m,
+                                                       const RankT *__restrict__ rank,
+                                                       const unsigned long long *__restrict__ bid, Control *ctrl,
+                                                       int32_t *__restrict__ match, int n) {
+  constexpr int kNone = 0x7FFFFFFF;
+  const int chains = ld_volatile_s32(&ctrl->coop_count);
+  if (chains <= 0 || ld_volatile_s32(&ctrl->status)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t *sbid = reinterpret_cast<uint32_t *>(smem_raw);
+  uint16_t *spos = reinterpret_cast<uint16_t *>(smem_raw + static_cast<size_t>(n) * 4);
+  // First candidate position of step t in s_best[t % 3]; -1: invalid input.
+  // Three buffers: after step t's barrier thread 0 clears the one step t + 2
+  // will use, which every thread finished reading before that barrier.
+  __shared__ int s_best[3];
+  __shared__ uint32_t s_old;
+  __shared__ unsigned long long s_props;
+  const int tid = threadIdx.x;
+  coop_load(bid, sbid, spos, n);
+  if (tid == 0) {
+    s_best[0] = s_best[1] = s_best[2] = kNone;
+    s_props = 0;
+  }
+  __syncthreads();
+  unsigned long long settled = 0;
+  unsigned int hops = 0;
+  int t = 0;
+  bool stop = false;
+  int per_start = 1;  // spans of 1024 a man's scan starts with: what the last one needed
+  for (int c = 0; c < chains && !stop; ++c) {
+    const int2 ch = ctrl->coop_chain[c];
+    int m = ch.x, pos = ch.y, per = per_start, from = pos;
+    while (pos < n) {
+      const int *row = pref_m + static_cast<size_t>(m) * n;
+      const RankT *rrow = rank + static_cast<size_t>(m) * n;
+      int wv[8];
+      uint32_t rv[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int r = pos + tid + 1024 * j;
+        wv[j] = (j < per && r < n) ? __ldg(row + r) : -1;
+      }
+      bool bad = false;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        rv[j] = 0xFFFFFFFFu;
+        if (wv[j] != -1) {
+          if (static_cast<unsigned>(wv[j]) < static_cast<unsigned>(n)) {
+            rv[j] = static_cast<uint32_t>(__ldg(rrow + wv[j]));
+          } else {
+            report(ctrl, kStatusInvalidInput, wv[j]);
+            bad = true;
+          }
+        }
+      }
+      int mine = bad ? -1 : kNone;
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (mine == kNone && rv[j] != 0xFFFFFFFFu && rv[j] < (sbid[wv[j]] >> 16)) mine = pos + tid + 1024 * j;
+      const int b = t % 3;
+      if (mine != kNone) atomicMin(&s_best[b], mine);
+      __syncthreads();
+      const int best = s_best[b];
+      if (tid == 0) s_best[(t + 2) % 3] = kNone;
+      ++t;
+      if (best < 0) {
+        stop = true;
+        break;
+      }
+      if (best == kNone) {  // rejected by every woman of the span
+        const int end = min(n, pos + 1024 * per);
+        settled += end - pos;
+        pos = end;
+        per = min(2 * per, 8);
+        continue;
+      }
+      // One thread records the proposal; the others read the result after
+      // the barrier, and the next proposal comes after the next step's
+      // barrier, so nothing is overwritten while it is read.
+      if (tid == 0) {
+        const int w = row[best];
+        const uint32_t rk = static_cast<uint32_t>(rrow[w]);
+        s_old = sbid[w];
+        sbid[w] = (rk << 16) | static_cast<uint32_t>(m);
+        spos[m] = static_cast<uint16_t>(best);
+      }
+      __syncthreads();
+      const uint32_t old = s_old;
+      settled += best - pos + 1;
+      hops++;
+      per_start = min(8, (best - from) / 1024 + 1);
+      if (old == 0xFFFFFFFFu) break;  // she was free: the chain ends
+      m = static_cast<int>(old & 0xFFFFu);
+      pos = spos[m] + 1;
+      from = pos;
+      per = per_start;
+    }
+    if (!stop && pos >= n && tid == 0) report(ctrl, kStatusInvalidInput, m);  // rejected by every woman
+  }
+  if (tid == 0) {
+    atomicAdd(&ctrl->tail_proposals, settled);
+    atomicAdd(&ctrl->tail_hops, hops);
+  }
+  __syncthreads();
+  if (ld_volatile_s32(&ctrl->status)) return;
+  if (tid == 0) ctrl->coop_count = 0;
   tail_finish(sbid, spos, match, n, ctrl, &s_props);
 }
 
@@ -1022,6 +1250,8 @@ __global__ void k_retry_reset(unsigned long long *bid, int n, Control *ctrl) {
     ctrl->tail_proposals = 0;
     ctrl->bulk_hops = 0;
     ctrl->tail_hops = 0;
+    ctrl->coop_count = 0;
+    ctrl->use_filter = 0;
   }
 }
 

@@ -95,6 +95,7 @@ constexpr int kStepHalt = 4;         // the caller's check asked to stop
 
 struct GlobalBids {
   using Word = unsigned long long;
+  static constexpr bool kFiltered = false;
   unsigned long long *bid;
   __device__ __forceinline__ Word word(int w) const { return ld_relaxed_u64(bid + w); }
   __device__ __forceinline__ static uint32_t rank_of(Word b) { return bid_rank(b); }
@@ -124,6 +125,7 @@ struct GlobalBids {
 
 struct SharedBids {
   using Word = uint32_t;
+  static constexpr bool kFiltered = false;
   uint32_t *sbid;  // rank << 16 | man; 0xFFFFFFFF = free
   uint16_t *spos;  // each man's position of his current proposal
   __device__ __forceinline__ Word word(int w) const { return lds_relaxed_u32(sbid + w); }
@@ -152,6 +154,62 @@ struct SharedBids {
     if (old == 0xFFFFFFFFu) return true;
     m = static_cast<int>(old & 0xFFFFu);
     pos = static_cast<int>(res >> 32);
+    return false;
+  }
+};
+
+// GlobalBids behind a per-CTA filter in shared memory: lrank[w] is an upper
+// bound on the rank of woman w's partner (all ones while unknown).  Every
+// value written to it is a rank her partner had or a rank a proposal to her
+// claimed, and her partner only ever improves, so it stays an upper bound
+// even when two warps race on it (a lost update only loosens it): plain
+// volatile loads and stores suffice.  A man she ranks above lrank[w] is
+// rejected without touching L2 (check); every bid word the CTA reads lowers
+// the bound (learn); a proposal first claims her locally, so only a warp that
+// beats every rank its CTA knows for her sends the global atomic.  Where the
+// men of many warps scan the same women (congested and correlated lists),
+// this turns one L2 read per proposal into about one per woman and CTA, and
+// the convoy of losing atomics on the first free woman into a few.
+struct FilteredBids {
+  using Word = unsigned long long;
+  static constexpr bool kFiltered = true;
+  unsigned long long *bid;
+  volatile uint32_t *lrank;
+  __device__ __forceinline__ Word word(int w) const { return ld_relaxed_u64(bid + w); }
+  __device__ __forceinline__ static uint32_t rank_of(Word b) { return bid_rank(b); }
+  __device__ __forceinline__ uint32_t cur_rank(int w) const { return bid_rank(ld_relaxed_u64(bid + w)); }
+  // No side effects, so the loads of several windows can be in flight at once.
+  __device__ __forceinline__ bool check(int w, uint32_t rk, Word &cw) const {
+    if (rk > lrank[w]) {
+      cw = kFree;
+      return false;
+    }
+    cw = __ldcg(bid + w);
+    return rk < bid_rank(cw);
+  }
+  __device__ __forceinline__ void learn(int w, Word cw) const {
+    const uint32_t r = bid_rank(cw);
+    if (r < lrank[w]) lrank[w] = r;
+  }
+  __device__ __forceinline__ bool holder(Word b, int &hm, int &hp) const {
+    if (b == kFree) return false;
+    hm = static_cast<int>(bid_man(b));
+    hp = static_cast<int>(bid_pos(b)) + 1;
+    return true;
+  }
+  __device__ __forceinline__ unsigned long long propose(int w, uint32_t rk, int m, int pos) const {
+    if (lrank[w] < rk) return 0ull;  // her partner is better than him already
+    lrank[w] = rk;
+    const unsigned long long old =
+        atomicMin(bid + w, pack_bid(rk, static_cast<uint32_t>(m), static_cast<uint32_t>(pos)));
+    if (bid_rank(old) > rk) return old;
+    learn(w, old);
+    return 0ull;
+  }
+  __device__ __forceinline__ bool decode(unsigned long long res, int &m, int &pos) const {
+    if (res == kFree) return true;
+    m = static_cast<int>(bid_man(res));
+    pos = static_cast<int>(bid_pos(res)) + 1;
     return false;
   }
 };
@@ -202,13 +260,22 @@ __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, cons
     if (kAhead) ahead.m = -1;
     const int st0 = finish_choice<kLdg, kManMajor>(raw, rank, K, n, query, m, r, w0, rk0);
     typename Bids::Word cw = 0;
-    uint32_t cr = 0u;
-    if (st0 == 0) {
-      cw = bids.word(w0);
-      cr = Bids::rank_of(cw);
+    unsigned cm;
+    if constexpr (Bids::kFiltered) {
+      bool cand = false;
+      if (st0 == 0) cand = bids.check(w0, rk0, cw);
+      if (!keep_going()) return kStepHalt;
+      cm = __ballot_sync(kFullMask, cand);
+      if (st0 == 0) bids.learn(w0, cw);
+    } else {
+      uint32_t cr = 0u;
+      if (st0 == 0) {
+        cw = bids.word(w0);
+        cr = Bids::rank_of(cw);
+      }
+      if (!keep_going()) return kStepHalt;
+      cm = __ballot_sync(kFullMask, st0 == 0 && rk0 < cr);
     }
-    if (!keep_going()) return kStepHalt;
-    unsigned cm = __ballot_sync(kFullMask, st0 == 0 && rk0 < cr);
     const unsigned em = (pos + 32 > K) ? __ballot_sync(kFullMask, st0 == 1 || st0 == 2) : 0u;
     if (em) cm &= (1u << (__ffs(em) - 1)) - 1u;
     // Issue the window of the man the first candidate would displace.
@@ -245,17 +312,40 @@ __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, cons
   // wide path
   int w[kMaxSub], st[kMaxSub];
   uint32_t rk[kMaxSub], cr[kMaxSub];
+  bool cd[kMaxSub];  // FilteredBids: candidate
+  if constexpr (Bids::kFiltered) {
+    typename Bids::Word cws[kMaxSub];
 #pragma unroll
-  for (int s = 0; s < kMaxSub; ++s) {
-    st[s] = 3;
-    w[s] = 0;
-    rk[s] = 0xFFFFFFFFu;
-    cr[s] = 0u;
-    if (s < S) {
-      const int r = pos + 32 * s + lane;
-      if (r < n) {
-        st[s] = load_choice<kLdg, kManMajor>(pref_m, rank, prefix, K, n, query, m, r, w[s], rk[s]);
-        if (st[s] == 0) cr[s] = bids.cur_rank(w[s]);
+    for (int s = 0; s < kMaxSub; ++s) {
+      st[s] = 3;
+      w[s] = 0;
+      rk[s] = 0xFFFFFFFFu;
+      cd[s] = false;
+      cws[s] = 0;
+      if (s < S) {
+        const int r = pos + 32 * s + lane;
+        if (r < n) {
+          st[s] = load_choice<kLdg, kManMajor>(pref_m, rank, prefix, K, n, query, m, r, w[s], rk[s]);
+          if (st[s] == 0) cd[s] = bids.check(w[s], rk[s], cws[s]);
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < kMaxSub; ++s)
+      if (st[s] == 0) bids.learn(w[s], cws[s]);
+  } else {
+#pragma unroll
+    for (int s = 0; s < kMaxSub; ++s) {
+      st[s] = 3;
+      w[s] = 0;
+      rk[s] = 0xFFFFFFFFu;
+      cr[s] = 0u;
+      if (s < S) {
+        const int r = pos + 32 * s + lane;
+        if (r < n) {
+          st[s] = load_choice<kLdg, kManMajor>(pref_m, rank, prefix, K, n, query, m, r, w[s], rk[s]);
+          if (st[s] == 0) cr[s] = bids.cur_rank(w[s]);
+        }
       }
     }
   }
@@ -267,7 +357,7 @@ __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, cons
     cm[s] = 0u;
     em[s] = 0u;
     if (s < S) {
-      cm[s] = __ballot_sync(kFullMask, st[s] == 0 && rk[s] < cr[s]);
+      cm[s] = __ballot_sync(kFullMask, Bids::kFiltered ? cd[s] : (st[s] == 0 && rk[s] < cr[s]));
       if (edge) em[s] = __ballot_sync(kFullMask, st[s] == 1 || st[s] == 2);
     }
   }

@@ -239,6 +239,25 @@ def test_bad_row_deep_in_the_inversion(ctx, n, row, defect, host):
         assert np.array_equal(to_host(match), want) and st["proposals"] == props
 
 
+@pytest.mark.parametrize("kind,n,param", [
+    (pb.SMP_GEN_CONGESTED, 4097, 0),      # men alike, women not: the bulk runs with its shared filter
+    (pb.SMP_GEN_REF_CONGESTED, 3001, 0),  # both sides alike: plain bulk, displacement-heavy tail
+    (pb.SMP_GEN_GROUPED, 3000, 3),
+    (pb.SMP_GEN_CORRELATED, 4096, 50),
+    (pb.SMP_GEN_SOLO, 1500, 0),           # one chain scanning deep: all of it in the CTA-wide tail
+])
+def test_deep_chain_families_match_oracle(ctx, kind, n, param):
+    # Rank-mode solves whose last chains k_tail hands to the CTA-wide tail
+    # kernel, one after another; the matching and the proposal count must not
+    # depend on that order.
+    pm, pw = ctx.generate(kind, n, seed=11, param=param)
+    match, st = ctx.solve(pm, pw, check=True)
+    want, props = oracle.gs_seq(to_host(pm), to_host(pw))
+    assert np.array_equal(to_host(match), want)
+    assert st["proposals"] == props
+    assert st["blocking_pairs"] == 0
+
+
 def test_bad_arguments(ctx):
     with pytest.raises(pb.SmpError) as e:
         ctx.generate(pb.SMP_GEN_SOLO, 2, seed=1)
