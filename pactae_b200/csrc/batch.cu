@@ -63,12 +63,13 @@ int launch_batch_t(smp_batch &b, cudaStream_t s, int grid, const int32_t *order,
 
 // Dynamic shared memory of the chosen kernel (set before any capture).
 int set_batch_attribute(smp_batch &b) {
+  const Ctx &c = b.ctx->c;
   cudaError_t e;
   switch (b.subs) {
-    case 1: e = cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b.smem)); break;
-    case 2: e = cudaFuncSetAttribute(k_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b.smem)); break;
-    case 4: e = cudaFuncSetAttribute(k_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b.smem)); break;
-    default: e = cudaFuncSetAttribute(k_batch<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(b.smem)); break;
+    case 1: e = allow_dynamic_smem(c, k_batch<1>); break;
+    case 2: e = allow_dynamic_smem(c, k_batch<2>); break;
+    case 4: e = allow_dynamic_smem(c, k_batch<4>); break;
+    default: e = allow_dynamic_smem(c, k_batch<8>); break;
   }
   return e == cudaSuccess ? SMP_OK : b.ctx->c.fail_cuda("k_batch smem attribute");
 }
@@ -220,22 +221,22 @@ int launch_batch_kernel(Ctx &c, cudaStream_t s, int subs, BatchInstance *table, 
   cudaError_t e = cudaSuccess;
   switch (subs) {
     case 1:
-      e = cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      e = allow_dynamic_smem(c, k_batch<1>);
       if (e == cudaSuccess)
         k_batch<1><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1, rank_smem_elems);
       break;
     case 2:
-      e = cudaFuncSetAttribute(k_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      e = allow_dynamic_smem(c, k_batch<2>);
       if (e == cudaSuccess)
         k_batch<2><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1, rank_smem_elems);
       break;
     case 4:
-      e = cudaFuncSetAttribute(k_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      e = allow_dynamic_smem(c, k_batch<4>);
       if (e == cudaSuccess)
         k_batch<4><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1, rank_smem_elems);
       break;
     default:
-      e = cudaFuncSetAttribute(k_batch<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      e = allow_dynamic_smem(c, k_batch<8>);
       if (e == cudaSuccess)
         k_batch<8><<<grid, block, smem, s>>>(table, order, count, queue, slabs, slab_elems, max_n, 1, rank_smem_elems);
       break;

@@ -6,6 +6,9 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
+#include <set>
+#include <utility>
 #include <array>
 #include <string>
 
@@ -155,6 +158,31 @@ struct Ctx {
     return SMP_ERR_CUDA;
   }
 };
+
+// Lets a kernel launch with as much dynamic shared memory as the device
+// allows beside its static shared memory.  The attribute is process-wide per
+// kernel, so it is set once per kernel and device, to that one value, and
+// never changed: setting it to each launch's own size would let a small
+// launch on one thread (a solve) lower it under a larger launch another
+// thread (the serving loop) is about to make, which then fails.
+inline cudaError_t allow_dynamic_smem_ptr(const Ctx &c, const void *kernel) {
+  static std::mutex mu;
+  static std::set<std::pair<const void *, int>> done;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(kernel, c.device);
+  if (done.count(key)) return cudaSuccess;
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, kernel);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(c.smem_optin - a.sharedSizeBytes));
+  if (e == cudaSuccess) done.insert(key);
+  return e;
+}
+template <typename Kernel>
+inline cudaError_t allow_dynamic_smem(const Ctx &c, Kernel kernel) {
+  return allow_dynamic_smem_ptr(c, reinterpret_cast<const void *>(kernel));
+}
 
 // smp_b200.cu: a whole solve split into its asynchronous part and its
 // completion (the public smp_b200_solve is the two with a sync between).

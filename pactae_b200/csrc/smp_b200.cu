@@ -85,7 +85,7 @@ int enqueue_validate(Ctx &c) {
     c.last_error = "validate: n too large for the shared-memory bitmap";
     return SMP_ERR_UNSUPPORTED;
   }
-  if (cudaFuncSetAttribute(k_validate_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+  if (allow_dynamic_smem(c, k_validate_rows) !=
       cudaSuccess)
     return c.fail_cuda("k_validate_rows smem attribute");
   const int grid = std::min(n, c.sm_count * 4);
@@ -137,8 +137,7 @@ int enqueue_invert(Ctx &c, const int32_t *pref_w, RankT *rank, int gate) {
   if constexpr (std::is_same<RankT, int32_t>::value) {
     const size_t smem16 = row_smem_bytes<uint16_t>(n);
     if (n <= kU16MaxN && smem16 <= c.smem_optin) {  // int32 output from a uint16 shared row
-      if (cudaFuncSetAttribute(k_invert_wide, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem16)) != cudaSuccess)
+      if (allow_dynamic_smem(c, k_invert_wide) != cudaSuccess)
         return c.fail_cuda("k_invert_wide smem attribute");
       int per_sm = 0;
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_invert_wide, 512, smem16) != cudaSuccess) {
@@ -153,8 +152,7 @@ int enqueue_invert(Ctx &c, const int32_t *pref_w, RankT *rank, int gate) {
   }
   const size_t smem = row_smem_bytes<RankT>(n);
   if (smem <= c.smem_optin) {
-    if (cudaFuncSetAttribute(k_invert<RankT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem)) != cudaSuccess)
+    if (allow_dynamic_smem(c, k_invert<RankT>) != cudaSuccess)
       return c.fail_cuda("k_invert smem attribute");
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_invert<RankT>, 512, smem) != cudaSuccess) {
@@ -239,7 +237,7 @@ int enqueue_qinvert(Ctx &c, int w0, int w1) {
   // larger n: the one with a clearing pass per row.
   const auto kernel = c.n <= kColorMaxN ? k_qinvert_c : k_qinvert;
   const size_t smem = row_smem_bytes<uint16_t>(c.n);
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+  if (allow_dynamic_smem(c, kernel) !=
       cudaSuccess)
     return c.fail_cuda("k_qinvert smem attribute");
   const int block = c.n <= kColorMaxN ? 256 : 512;
@@ -303,7 +301,7 @@ int launch_bulk(Ctx &c, int round) {
     int rc = c.check_launch("k_wdistinct");
     if (rc) return rc;
     const auto kernel = k_bulk<RankT, kSub, true>;
-    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(filter)) !=
+    if (allow_dynamic_smem(c, kernel) !=
         cudaSuccess)
       return c.fail_cuda("k_bulk smem attribute");
     int per_sm = 0;
@@ -330,9 +328,7 @@ int launch_tail(Ctx &c, int round, int only_mode) {
   const RankT *rank = reinterpret_cast<const RankT *>(c.d_rankT.ptr);  // man-major
   const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
   const size_t smem = tail_smem_bytes(c.n);
-  if (cudaFuncSetAttribute(k_tail<RankT, kSub>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem)) != cudaSuccess)
-    return c.fail_cuda("k_tail smem attribute");
+  if (allow_dynamic_smem(c, k_tail<RankT, kSub>) != cudaSuccess) return c.fail_cuda("k_tail smem attribute");
   k_tail<RankT, kSub><<<1, 1024, smem, c.stream>>>(c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(),
                                                    c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
                                                    c.d_match.as<int32_t>(), c.n, round, only_mode, kCoopChains);
@@ -340,8 +336,7 @@ int launch_tail(Ctx &c, int round, int only_mode) {
   int rc = c.check_launch("k_tail");
   if (rc) return rc;
   // the last chains, if k_tail handed them over
-  if (cudaFuncSetAttribute(k_tail_coop<RankT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem)) != cudaSuccess)
+  if (allow_dynamic_smem(c, k_tail_coop<RankT>) != cudaSuccess)
     return c.fail_cuda("k_tail_coop smem attribute");
   k_tail_coop<RankT><<<1, 1024, smem, c.stream>>>(c.pref_m, rank, c.d_bid.as<unsigned long long>(),
                                                   c.d_ctrl.as<Control>(), c.d_match.as<int32_t>(), c.n);
@@ -351,7 +346,7 @@ int launch_tail(Ctx &c, int round, int only_mode) {
 
 int launch_tail_query(Ctx &c) {
   const size_t smem = tail_smem_bytes(c.n);
-  if (cudaFuncSetAttribute(k_tail_q, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+  if (allow_dynamic_smem(c, k_tail_q) !=
       cudaSuccess)
     return c.fail_cuda("k_tail_q smem attribute");
   k_tail_q<<<1, 1024, smem, c.stream>>>(c.pref_m, c.d_prefix.as<uint32_t>(), c.K, c.d_bid.as<unsigned long long>(),

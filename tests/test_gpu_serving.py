@@ -77,3 +77,28 @@ def test_oversize_request_is_refused(ctx):
         with pytest.raises(pb.SmpError) as e:
             srv.submit(pm, pw, torch.empty(101, dtype=torch.int32, device="cuda:0"))
         assert e.value.status == pb.SMP_ERR_BUSY
+
+
+def test_solves_beside_the_server(ctx):
+    # Kernels with dynamic shared memory are launched from the caller's thread
+    # (solves) and the server's thread at once, each with its own size.  A
+    # launch must not fail because the other thread set the kernel's shared
+    # memory limit for a smaller launch just before.
+    import numpy as np
+
+    big = make_requests(ctx, 8, seed=21, n_lo=700, n_hi=1600)
+    small = make_requests(ctx, 12, seed=22, n_lo=40, n_hi=300)
+    alone = [ctx.solve(pm, pw) for pm, pw, _ in big]
+    with pb.Server(route_n=256) as srv:
+        tickets = [srv.submit(pm, pw, mt) for pm, pw, mt in big]
+        with pb.Context() as other:
+            for _ in range(3):
+                for pm, pw, _ in small:
+                    m1, _ = other.solve(pm, pw)
+                    m2, _ = other.solve(pm.cpu().numpy(), pw.cpu().numpy())
+                    assert np.array_equal(m1.cpu().numpy(), m2)
+        for t, (want, wst), (_, _, mt) in zip(tickets, alone, big):
+            res = srv.poll(t)
+            assert res["status"] == 0
+            assert np.array_equal(mt.cpu().numpy(), want.cpu().numpy())
+            assert res["proposals"] == wst["proposals"]
