@@ -39,6 +39,91 @@ __host__ __device__ constexpr size_t batch_smem_bytes(int max_n) {
   return (static_cast<size_t>(max_n) * 4 + static_cast<size_t>(max_n) * 2 + 15) & ~static_cast<size_t>(15);
 }
 
+// Slab inversion in groups of rows through the shared rank region (free
+// while the instance's matrix lives in the slab).  Scattering each woman's
+// row straight into the slab cost a random 2-byte store and a random
+// read-back per entry, two L2 sector transactions each: about 70 % of a
+// batch.  Here the CTA takes G women at a time, G = rows of `slots` (16-byte
+// aligned, with room for the destination's offset) that fit the region, at
+// most one per warp; each woman's warps stream her row with 16-byte loads and
+// scatter it into her shared row, placed at the destination row's offset from
+// a 16-byte boundary; then all threads write the group out with 16-byte
+// stores, checking that no slot stayed unset (a row that is not a
+// permutation).
+__device__ __forceinline__ int batch_row_slots(int n) { return ((n + 7) / 8) * 8 + 8; }
+
+__device__ __forceinline__ void batch_scatter(uint16_t *srow, int m, int r, int n, bool &bad) {
+  if (static_cast<unsigned>(m) < static_cast<unsigned>(n)) {
+    srow[m] = static_cast<uint16_t>(r);
+  } else {
+    bad = true;
+  }
+}
+
+__device__ __forceinline__ void batch_invert_slab(const int32_t *__restrict__ pref_w, uint16_t *slab, int n, int G,
+                                                  uint16_t *buf, bool &bad) {
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;
+  const int warp = tid >> 5;
+  const int wpr = (nthr >> 5) / G;  // warps per woman
+  const int g = warp / wpr;         // this warp's woman in the group (g >= G: none)
+  const int sub = (warp % wpr) * 32 + (tid & 31);
+  const int subn = wpr * 32;
+  const int rs = batch_row_slots(n);
+  const int cmax = rs / 8;
+  uint4 *b4 = reinterpret_cast<uint4 *>(buf);
+  for (int w0 = 0; w0 < n; w0 += G) {
+    for (int c = tid; c < G * cmax; c += nthr) b4[c] = make_uint4(~0u, ~0u, ~0u, ~0u);
+    __syncthreads();
+    const int w = w0 + g;
+    if (g < G && w < n) {
+      const int32_t *row = pref_w + static_cast<size_t>(w) * n;
+      const int pre = static_cast<int>((reinterpret_cast<uintptr_t>(slab + static_cast<size_t>(w) * n) & 15u) >> 1);
+      uint16_t *srow = buf + g * rs + pre;
+      const int head = min(n, static_cast<int>(((16u - (reinterpret_cast<uintptr_t>(row) & 15u)) & 15u) >> 2));
+      if (sub < head) batch_scatter(srow, __ldcs(row + sub), sub, n, bad);
+      const int nq = (n - head) >> 2;
+      const int4 *rq = reinterpret_cast<const int4 *>(row + head);
+      for (int i = sub; i < nq; i += subn) {
+        const int4 q = __ldcs(rq + i);
+        const int r = head + 4 * i;
+        batch_scatter(srow, q.x, r, n, bad);
+        batch_scatter(srow, q.y, r + 1, n, bad);
+        batch_scatter(srow, q.z, r + 2, n, bad);
+        batch_scatter(srow, q.w, r + 3, n, bad);
+      }
+      for (int t = head + 4 * nq + sub; t < n; t += subn) batch_scatter(srow, __ldcs(row + t), t, n, bad);
+    }
+    __syncthreads();
+    for (int idx = tid; idx < G * cmax; idx += nthr) {
+      const int gg = idx / cmax, c = idx - gg * cmax;
+      const int ww = w0 + gg;
+      if (ww >= n) continue;
+      uint16_t *out = slab + static_cast<size_t>(ww) * n;
+      const int pre = static_cast<int>((reinterpret_cast<uintptr_t>(out) & 15u) >> 1);
+      if (c >= (pre + n + 7) / 8) continue;
+      const uint4 v = b4[gg * cmax + c];
+      const int first = c * 8 - pre;  // row element in the chunk's first slot
+      if (first >= 0 && first + 8 <= n) {
+        bad |= (__vcmpeq2(v.x, 0xFFFFFFFFu) | __vcmpeq2(v.y, 0xFFFFFFFFu) | __vcmpeq2(v.z, 0xFFFFFFFFu) |
+                __vcmpeq2(v.w, 0xFFFFFFFFu)) != 0u;
+        reinterpret_cast<uint4 *>(out - pre)[c] = v;
+      } else {
+        const uint16_t *vals = reinterpret_cast<const uint16_t *>(&v);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int e = first + k;
+          if (e >= 0 && e < n) {
+            bad |= vals[k] == 0xFFFFu;
+            out[e] = vals[k];
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // rank_smem_elems: uint16 slots of shared memory after the bids; an instance
 // whose n*n rank matrix fits there keeps it on chip (small instances), the
 // others use the CTA's slab in global memory.
@@ -89,9 +174,13 @@ __global__ void __launch_bounds__(512, 2) k_batch(BatchInstance *__restrict__ ta
     }
     __syncthreads();
 
-    // 1. inversion, one row per warp, checked by reading the row back
+    // 1. inversion: through the shared region in groups of rows when the
+    // matrix lives in the slab, else one row per warp, checked by reading
+    // the row back
     bool bad = false;
-    for (int w = warp; w < n; w += nwarps) {
+    const int groups = rank == slab ? min(rank_smem_elems / batch_row_slots(n), nwarps) : 0;
+    if (groups >= 1) batch_invert_slab(pref_w, slab, n, groups, srank, bad);
+    for (int w = groups >= 1 ? n : warp; w < n; w += nwarps) {
       const int32_t *row = pref_w + static_cast<size_t>(w) * n;
       uint16_t *out = rank + static_cast<size_t>(w) * n;
       for (int r = lane; r < n; r += 32) {
