@@ -978,22 +978,27 @@ __global__ void __launch_bounds__(1024, 1) k_tail_coop(const int32_t *__restrict
                                                        const RankT *__restrict__ rank,
                                                        const unsigned long long *__restrict__ bid, Control *ctrl,
                                                        int32_t *__restrict__ match, int n) {
-  constexpr int kNone = 0x7FFFFFFF;
+  constexpr unsigned long long kNone = ~0ull;
   const int chains = ld_volatile_s32(&ctrl->coop_count);
   if (chains <= 0 || ld_volatile_s32(&ctrl->status)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint32_t *sbid = reinterpret_cast<uint32_t *>(smem_raw);
   uint16_t *spos = reinterpret_cast<uint16_t *>(smem_raw + static_cast<size_t>(n) * 4);
-  // First candidate position of step t in s_best[t % 3]; -1: invalid input.
-  // Three buffers: after step t's barrier thread 0 clears the one step t + 2
-  // will use, which every thread finished reading before that barrier.
-  __shared__ int s_best[3];
-  __shared__ uint32_t s_old;
+  // Step t's first candidate in s_best[t % 3] as position << 32 | her bid
+  // word when it was read, so every thread learns from the minimum whom she
+  // drops; s_bad[t % 3]: an invalid entry was seen.  Three buffers: after
+  // step t's barrier thread 0 clears the ones step t + 2 will use, which
+  // every thread finished reading before that barrier.
+  __shared__ unsigned long long s_best[3];
+  __shared__ int s_bad[3];
   __shared__ unsigned long long s_props;
   const int tid = threadIdx.x;
   coop_load(bid, sbid, spos, n);
   if (tid == 0) {
-    s_best[0] = s_best[1] = s_best[2] = kNone;
+    for (int i = 0; i < 3; ++i) {
+      s_best[i] = kNone;
+      s_bad[i] = 0;
+    }
     s_props = 0;
   }
   __syncthreads();
@@ -1001,20 +1006,37 @@ __global__ void __launch_bounds__(1024, 1) k_tail_coop(const int32_t *__restrict
   unsigned int hops = 0;
   int t = 0;
   bool stop = false;
+  // Thread 0 records a proposal at the start of the next step, before that
+  // step's barrier: the other threads took her old bid word from the
+  // minimum, and the next man's span does not contain her (he scans his list
+  // after her), so nothing reads her word or the proposer's position
+  // meanwhile, and every step after sees them.
+  bool pend = false;
+  int pend_w = 0, pend_m = 0, pend_pos = 0;
+  uint32_t pend_val = 0;
   int per_start = 1;  // spans of 1024 a man's scan starts with: what the last one needed
+  int wv[8];
   for (int c = 0; c < chains && !stop; ++c) {
     const int2 ch = ctrl->coop_chain[c];
     int m = ch.x, pos = ch.y, per = per_start, from = pos;
+    bool loaded = false;  // wv holds the span [pos, pos + 1024 per) of man m
     while (pos < n) {
+      if (tid == 0 && pend) {
+        sbid[pend_w] = pend_val;
+        spos[pend_m] = static_cast<uint16_t>(pend_pos);
+        pend = false;
+      }
       const int *row = pref_m + static_cast<size_t>(m) * n;
       const RankT *rrow = rank + static_cast<size_t>(m) * n;
-      int wv[8];
-      uint32_t rv[8];
+      if (!loaded) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int r = pos + tid + 1024 * j;
-        wv[j] = (j < per && r < n) ? __ldg(row + r) : -1;
+        for (int j = 0; j < 8; ++j) {
+          const int r = pos + tid + 1024 * j;
+          wv[j] = (j < per && r < n) ? __ldg(row + r) : -1;
+        }
       }
+      loaded = false;
+      uint32_t rv[8];
       bool bad = false;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
@@ -1028,49 +1050,84 @@ __global__ void __launch_bounds__(1024, 1) k_tail_coop(const int32_t *__restrict
           }
         }
       }
-      int mine = bad ? -1 : kNone;
+      unsigned long long mine = kNone;
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
-        if (mine == kNone && rv[j] != 0xFFFFFFFFu && rv[j] < (sbid[wv[j]] >> 16)) mine = pos + tid + 1024 * j;
+      for (int j = 0; j < 8; ++j) {
+        if (mine == kNone && rv[j] != 0xFFFFFFFFu) {
+          const uint32_t cur = sbid[wv[j]];
+          if (rv[j] < (cur >> 16))
+            mine = (static_cast<unsigned long long>(pos + tid + 1024 * j) << 32) | cur;
+        }
+      }
       const int b = t % 3;
-      if (mine != kNone) atomicMin(&s_best[b], mine);
+      if (bad) s_bad[b] = 1;
+      // one atomic per warp: positions are distinct, so one lane holds its minimum
+      const uint32_t at = mine == kNone ? 0xFFFFFFFFu : static_cast<uint32_t>(mine >> 32);
+      const uint32_t warp_min = __reduce_min_sync(kFullMask, at);  // every lane takes part
+      if (mine != kNone && at == warp_min) atomicMin(&s_best[b], mine);
       __syncthreads();
-      const int best = s_best[b];
-      if (tid == 0) s_best[(t + 2) % 3] = kNone;
+      const unsigned long long key = s_best[b];
+      const bool any_bad = s_bad[b] != 0;
+      if (tid == 0) {
+        s_best[(t + 2) % 3] = kNone;
+        s_bad[(t + 2) % 3] = 0;
+      }
       ++t;
-      if (best < 0) {
+      if (any_bad) {
         stop = true;
         break;
       }
-      if (best == kNone) {  // rejected by every woman of the span
+      if (key == kNone) {  // rejected by every woman of the span
         const int end = min(n, pos + 1024 * per);
         settled += end - pos;
         pos = end;
         per = min(2 * per, 8);
         continue;
       }
-      // One thread records the proposal; the others read the result after
-      // the barrier, and the next proposal comes after the next step's
-      // barrier, so nothing is overwritten while it is read.
-      if (tid == 0) {
-        const int w = row[best];
-        const uint32_t rk = static_cast<uint32_t>(rrow[w]);
-        s_old = sbid[w];
-        sbid[w] = (rk << 16) | static_cast<uint32_t>(m);
-        spos[m] = static_cast<uint16_t>(best);
-      }
-      __syncthreads();
-      const uint32_t old = s_old;
+      const int best = static_cast<int>(key >> 32);
+      const uint32_t old = static_cast<uint32_t>(key);
       settled += best - pos + 1;
       hops++;
       per_start = min(8, (best - from) / 1024 + 1);
-      if (old == 0xFFFFFFFFu) break;  // she was free: the chain ends
+      if (tid == 0) {
+        pend_w = row[best];
+        pend_val = (static_cast<uint32_t>(rrow[pend_w]) << 16) | static_cast<uint32_t>(m);
+        pend_m = m;
+        pend_pos = best;
+        pend = true;
+      }
+      if (old == 0xFFFFFFFFu) {  // she was free: the chain ends; the next one must see her taken
+        if (tid == 0) {
+          sbid[pend_w] = pend_val;
+          spos[pend_m] = static_cast<uint16_t>(pend_pos);
+          pend = false;
+        }
+        __syncthreads();
+        break;
+      }
+      // the man she drops: issue his first span at once
       m = static_cast<int>(old & 0xFFFFu);
+      if (m >= n) {  // not a man: the shared state is corrupt
+        if (tid == 0) report(ctrl, kStatusInvalidInput, m);
+        stop = true;
+        break;
+      }
       pos = spos[m] + 1;
       from = pos;
       per = per_start;
+      const int *nrow = pref_m + static_cast<size_t>(m) * n;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int r = pos + tid + 1024 * j;
+        wv[j] = (j < per && r < n) ? __ldg(nrow + r) : -1;
+      }
+      loaded = true;
     }
     if (!stop && pos >= n && tid == 0) report(ctrl, kStatusInvalidInput, m);  // rejected by every woman
+  }
+  if (tid == 0 && pend) {
+    sbid[pend_w] = pend_val;
+    spos[pend_m] = static_cast<uint16_t>(pend_pos);
   }
   if (tid == 0) {
     atomicAdd(&ctrl->tail_proposals, settled);
