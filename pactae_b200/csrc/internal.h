@@ -121,7 +121,7 @@ struct Ctx {
   bool tail_ran = false;
   int phase = 0;            // 0 staged, 1 prechecked, 2 inited, 3 cored, 4 posted
 
-  DeviceBuf d_pref_m, d_pref_w, d_rank, d_rankT, d_prefix, d_bid, d_tailq, d_seen, d_ctrl, d_match;
+  DeviceBuf d_pref_m, d_pref_w, d_rank, d_rankT, d_pr, d_prefix, d_bid, d_tailq, d_seen, d_ctrl, d_match;
   DeviceBuf d_husband, d_prank;
   DeviceBuf d_qcnt, d_qlist;
   DeviceBuf gen_keys_a, gen_keys_b, gen_seg, gen_temp, gen_aux;
@@ -132,8 +132,8 @@ struct Ctx {
   static constexpr int kCopyChunks = 16;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_chunk[kCopyChunks] = {};
-  std::array<DeviceBuf *, 19> buffers() {
-    return {&d_pref_m, &d_pref_w, &d_rank,    &d_rankT,    &d_prefix, &d_bid,    &d_tailq,
+  std::array<DeviceBuf *, 20> buffers() {
+    return {&d_pref_m, &d_pref_w, &d_rank,    &d_rankT,    &d_pr,     &d_prefix, &d_bid,    &d_tailq,
             &d_seen,   &d_ctrl,   &d_match,   &d_husband,  &d_prank,  &d_qcnt,   &d_qlist,
             &gen_keys_a, &gen_keys_b, &gen_seg, &gen_temp, &gen_aux};
   }

@@ -199,7 +199,28 @@ int enqueue_rank(Ctx &c, int gate) {
     k_transpose<int32_t><<<grid, 512, 0, c.stream>>>(c.d_rank.as<int32_t>(), c.d_rankT.as<int32_t>(), c.n,
                                                      c.d_ctrl.as<Control>(), gate);
   c.launches++;
-  return c.check_launch("k_transpose");
+  rc = c.check_launch("k_transpose");
+  if (rc || c.rank_bytes != 2) return rc;
+  // uint16 ranks: proposals read them by position (pr)
+  rc = c.d_pr.ensure(static_cast<size_t>(c.n) * c.n * 2);
+  if (rc) return rc;
+  const size_t smem = row_smem_bytes<uint16_t>(c.n);
+  if (allow_dynamic_smem(c, k_pr) != cudaSuccess) return c.fail_cuda("k_pr smem attribute");
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pr, 512, smem) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  k_pr<<<std::min(c.n, c.sm_count * std::max(per_sm, 1)), 512, smem, c.stream>>>(
+      c.pref_m, c.d_rankT.as<uint16_t>(), c.d_pr.as<uint16_t>(), c.n, c.d_ctrl.as<Control>(), gate);
+  c.launches++;
+  return c.check_launch("k_pr");
+}
+
+// The matrix rank-mode proposals read, as rank_layout<RankT>() says.
+template <typename RankT>
+const RankT *proposal_ranks(const Ctx &c) {
+  return reinterpret_cast<const RankT *>(rank_layout<RankT>() == 2 ? c.d_pr.ptr : c.d_rankT.ptr);
 }
 
 int enqueue_prefix_gather(Ctx &c, int gate) {
@@ -290,7 +311,7 @@ int enqueue_init(Ctx &c) {
 
 template <typename RankT, int kSub>
 int launch_bulk(Ctx &c, int round) {
-  const RankT *rank = reinterpret_cast<const RankT *>(c.d_rankT.ptr);  // man-major
+  const RankT *rank = proposal_ranks<RankT>(c);
   const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
   const int rank_threshold = c.tail_threshold > 0 ? std::min(c.tail_threshold, c.tail_threshold_rank) : 0;
   const size_t filter = sizeof(uint32_t) * static_cast<size_t>(c.n);
@@ -325,7 +346,7 @@ int launch_bulk(Ctx &c, int round) {
 
 template <typename RankT, int kSub>
 int launch_tail(Ctx &c, int round, int only_mode) {
-  const RankT *rank = reinterpret_cast<const RankT *>(c.d_rankT.ptr);  // man-major
+  const RankT *rank = proposal_ranks<RankT>(c);
   const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
   const size_t smem = tail_smem_bytes(c.n);
   if (allow_dynamic_smem(c, k_tail<RankT, kSub>) != cudaSuccess) return c.fail_cuda("k_tail smem attribute");
@@ -593,6 +614,7 @@ int reserve_buffers(Ctx &c, int32_t n) {
   if (!rc) rc = c.d_seen.ensure(((static_cast<size_t>(n) + 31) / 32) * 4);
   if (!rc) rc = init_buffers(c);
   if (!rc) rc = c.d_rankT.ensure(nn * c.rank_bytes);
+  if (!rc && c.rank_bytes == 2) rc = c.d_pr.ensure(nn * 2);
   if (!rc && c.query_ok) rc = c.d_qcnt.ensure(sizeof(int32_t) * static_cast<size_t>(n));
   if (!rc && c.query_ok)
     rc = c.d_qlist.ensure(sizeof(uint32_t) * static_cast<size_t>(n) * query_capacity(n, c.K));

@@ -638,6 +638,81 @@ __global__ void __launch_bounds__(256) k_qinvert_c(const int32_t *__restrict__ p
   if (bad) report(ctrl, kStatusInvalidInput, -1);
 }
 
+// The layout rank-mode proposals read: by position (pr, uint16 ranks, n <=
+// 65535) or man-major (rankT, int32 ranks).
+template <typename RankT>
+__host__ __device__ constexpr int rank_layout() {
+  return std::is_same<RankT, uint16_t>::value ? 2 : 1;
+}
+
+// ---------------------------------------------------------------------------
+// pr[m][r] = rankT[m][pref_m[m][r]]: the rank of man m in the list of his
+// r-th choice, in the order he proposes (what the reference's PR matrix
+// holds, kernel.cu:688-709, in uint16 and without the woman beside it).  A
+// proposal then reads pref_m[m][r] and pr[m][r] side by side, sequentially,
+// instead of a random rankT[m][w] that waits for pref_m[m][r]; in congested
+// and correlated lists, where men reject hundreds of women per acceptance,
+// that halves the round trips of a window.  One CTA per man row at a time:
+// his rankT row is staged in shared memory (16-byte loads over its aligned
+// interior), his pref_m row streams in with 16-byte loads and gathers from
+// it.  An out-of-range woman is reported.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) k_pr(const int32_t *__restrict__ pref_m, const uint16_t *__restrict__ rankT,
+                                            uint16_t *__restrict__ pr, int n, Control *ctrl, int gate) {
+  if (!gate_open(gate, ctrl)) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;
+  bool bad = false;
+  for (int m = blockIdx.x; m < n; m += gridDim.x) {
+    const uint16_t *src = rankT + static_cast<size_t>(m) * n;
+    const int pre = static_cast<int>((reinterpret_cast<uintptr_t>(src) & 15u) >> 1);
+    uint16_t *srow = reinterpret_cast<uint16_t *>(smem_raw) + pre;  // same offset from 16 bytes as src
+    const int a0 = min(n, (8 - pre) & 7);                           // first element on a 16-byte boundary
+    const int nch = (n - a0) >> 3;
+    for (int e = tid; e < a0; e += nthr) srow[e] = src[e];
+    for (int c = tid; c < nch; c += nthr)
+      reinterpret_cast<uint4 *>(srow + a0)[c] = __ldcs(reinterpret_cast<const uint4 *>(src + a0) + c);
+    for (int e = a0 + 8 * nch + tid; e < n; e += nthr) srow[e] = src[e];
+    __syncthreads();
+    const RowSpan s = row_span(pref_m, m, n);
+    uint16_t *out = pr + static_cast<size_t>(m) * n;
+    const auto gather = [&](int w, int r) {
+      if (static_cast<unsigned>(w) < static_cast<unsigned>(n)) {
+        out[r] = srow[w];
+      } else {
+        bad = true;
+      }
+    };
+    if (tid < s.head) gather(__ldcs(s.row + tid), tid);
+    // 8-byte stores when the four outputs of a 16-byte load line up (they do
+    // whenever pref_m starts on a 16-byte boundary); else one at a time
+    const bool wide = ((reinterpret_cast<uintptr_t>(out + s.head)) & 7u) == 0;
+    const auto rank_or_flag = [&](int w) -> uint32_t {
+      if (static_cast<unsigned>(w) < static_cast<unsigned>(n)) return srow[w];
+      bad = true;
+      return 0u;
+    };
+    for (int i = tid; i < s.nq; i += nthr) {
+      const int4 q = __ldcs(s.rq + i);
+      const int r = s.head + 4 * i;
+      if (wide) {
+        const uint2 v = make_uint2(rank_or_flag(q.x) | (rank_or_flag(q.y) << 16),
+                                   rank_or_flag(q.z) | (rank_or_flag(q.w) << 16));
+        *reinterpret_cast<uint2 *>(out + r) = v;
+      } else {
+        gather(q.x, r);
+        gather(q.y, r + 1);
+        gather(q.z, r + 2);
+        gather(q.w, r + 3);
+      }
+    }
+    if (tid < s.tail) gather(__ldcs(s.row + s.head + 4 * s.nq + tid), s.head + 4 * s.nq + tid);
+    __syncthreads();
+  }
+  if (bad) report(ctrl, kStatusInvalidInput, -1);
+}
+
 // ---------------------------------------------------------------------------
 // Bulk proposals on every SM.  Each warp carries one free man at a time
 // (man_step above, 64-bit bids in HBM).  A man accepted by a free woman
@@ -745,7 +820,8 @@ __global__ void __launch_bounds__(kFilter ? kFilterBlock : 256)
     if (lane == 0) free_now = ld_relaxed_s32(&ctrl->free_count);  // consumed after the window loads
     const int hold_m = m, hold_pos = pos;
     const auto keep_going = [&]() { return __shfl_sync(kFullMask, free_now, 0) > tail_threshold; };
-    const int rc = man_step<kMaxSub, true, true, 1, true>(bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m,
+    const int rc = man_step<kMaxSub, true, true, 1, rank_layout<RankT>()>(bids, keep_going, pref_m, rank, prefix, K, n,
+                                                                         query, lane, m,
                                                          pos, S, ahead, settled,
                                      hops, bad_value);
     if (rc == kStepMoved) continue;
@@ -934,7 +1010,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail(const int32_t *__restrict__ pr
         break;
       }
     }
-    const int rc = man_step<kMaxSub, (kMaxSub < 8), true, (kMaxSub == 8 ? 8 : 1), true>(
+    const int rc = man_step<kMaxSub, (kMaxSub < 8), true, (kMaxSub == 8 ? 8 : 1), rank_layout<RankT>()>(
         bids, keep_going, pref_m, rank, prefix, K, n, query, lane, m, pos, S, ahead, settled,
                                      hops, bad_value);
     if (rc == kStepMatchedFree && lane == 0) atomicSub(&s_busy, 1);
@@ -979,6 +1055,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail_coop(const int32_t *__restrict
                                                        const unsigned long long *__restrict__ bid, Control *ctrl,
                                                        int32_t *__restrict__ match, int n) {
   constexpr unsigned long long kNone = ~0ull;
+  constexpr bool kByPos = rank_layout<RankT>() == 2;  // rank: pr[m][r], else rankT[m][w]
   const int chains = ld_volatile_s32(&ctrl->coop_count);
   if (chains <= 0 || ld_volatile_s32(&ctrl->status)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1043,7 +1120,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail_coop(const int32_t *__restrict
         rv[j] = 0xFFFFFFFFu;
         if (wv[j] != -1) {
           if (static_cast<unsigned>(wv[j]) < static_cast<unsigned>(n)) {
-            rv[j] = static_cast<uint32_t>(__ldg(rrow + wv[j]));
+            rv[j] = static_cast<uint32_t>(__ldg(rrow + (kByPos ? pos + tid + 1024 * j : wv[j])));
           } else {
             report(ctrl, kStatusInvalidInput, wv[j]);
             bad = true;
@@ -1091,7 +1168,7 @@ __global__ void __launch_bounds__(1024, 1) k_tail_coop(const int32_t *__restrict
       per_start = min(8, (best - from) / 1024 + 1);
       if (tid == 0) {
         pend_w = row[best];
-        pend_val = (static_cast<uint32_t>(rrow[pend_w]) << 16) | static_cast<uint32_t>(m);
+        pend_val = (static_cast<uint32_t>(rrow[kByPos ? best : pend_w]) << 16) | static_cast<uint32_t>(m);
         pend_m = m;
         pend_pos = best;
         pend = true;

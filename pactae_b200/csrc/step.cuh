@@ -31,9 +31,13 @@ __device__ __forceinline__ uint32_t issue_choice(const int32_t *__restrict__ pre
 
 // kLdg: the rank matrix is in global memory and read through the read-only
 // path; false when it may be in shared memory (the batch kernel).
-// kManMajor: the matrix is stored man-major (rank[m][w] = her rank of him),
-// so a man's scan stays within his own row; else woman-major (rank[w][m]).
-template <bool kLdg = true, bool kManMajor = false, typename RankT>
+// kManMajor, the layout of the matrix a rank is read from:
+//   0 (false)  woman-major, rank[w][m] = her rank of him;
+//   1 (true)   man-major, rank[m][w], so a man's scan stays within his row;
+//   2          by position, pr[m][r] = the rank of man m in the list of his
+//              r-th choice: read at the index of his pref_m entry, so its
+//              load does not wait for that one.
+template <bool kLdg = true, int kManMajor = 0, typename RankT>
 __device__ __forceinline__ int finish_choice(uint32_t raw, const RankT *__restrict__ rank, int K, int n, bool query,
                                              int m, int r, int &w, uint32_t &rk) {
   if (r >= n) return 3;
@@ -45,12 +49,14 @@ __device__ __forceinline__ int finish_choice(uint32_t raw, const RankT *__restri
   if (query) return 1;
   w = static_cast<int>(raw);
   if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) return 2;
-  const RankT *p = kManMajor ? rank + static_cast<size_t>(m) * n + w : rank + static_cast<size_t>(w) * n + m;
+  const RankT *p = kManMajor == 2   ? rank + static_cast<size_t>(m) * n + r
+                   : kManMajor == 1 ? rank + static_cast<size_t>(m) * n + w
+                                    : rank + static_cast<size_t>(w) * n + m;
   rk = static_cast<uint32_t>(kLdg ? __ldg(p) : *p);
   return 0;
 }
 
-template <bool kLdg = true, bool kManMajor = false, typename RankT>
+template <bool kLdg = true, int kManMajor = 0, typename RankT>
 __device__ __forceinline__ int load_choice(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank,
                                            const uint32_t *__restrict__ prefix, int K, int n, bool query, int m,
                                            int r, int &w, uint32_t &rk) {
@@ -244,7 +250,7 @@ __device__ __forceinline__ int try_window(const Bids &bids, int lane, int w, uin
 
 // kSReset: the look-ahead (in windows) a man starts with after a move; 1 for
 // chains that end within a few choices, kMaxSub where displaced men scan deep.
-template <int kMaxSub, bool kAhead = true, bool kLdg = true, int kSReset = 1, bool kManMajor = false,
+template <int kMaxSub, bool kAhead = true, bool kLdg = true, int kSReset = 1, int kManMajor = 0,
           typename RankT, typename Bids, typename Check>
 __device__ __forceinline__ int man_step(const Bids &bids, Check keep_going, const int32_t *__restrict__ pref_m,
                                         const RankT *__restrict__ rank, const uint32_t *__restrict__ prefix, int K,
