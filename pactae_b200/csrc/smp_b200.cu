@@ -212,7 +212,8 @@ int enqueue_rank(Ctx &c, int gate) {
     per_sm = 1;
   }
   k_pr<<<std::min(c.n, c.sm_count * std::max(per_sm, 1)), 512, smem, c.stream>>>(
-      c.pref_m, c.d_rankT.as<uint16_t>(), c.d_pr.as<uint16_t>(), c.n, c.d_ctrl.as<Control>(), gate);
+      c.pref_m, c.d_rankT.as<uint16_t>(), c.d_pr.as<uint16_t>(), c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr,
+      c.K > 0 ? c.K : 0, c.n, c.d_ctrl.as<Control>(), gate);
   c.launches++;
   return c.check_launch("k_pr");
 }
@@ -224,7 +225,7 @@ const RankT *proposal_ranks(const Ctx &c) {
 }
 
 int enqueue_prefix_gather(Ctx &c, int gate) {
-  if (c.K <= 0) return SMP_OK;
+  if (c.K <= 0 || c.rank_bytes == 2) return SMP_OK;  // uint16 ranks: k_pr wrote the prefix
   const int n = c.n;
   const size_t total = static_cast<size_t>(n) * c.K;
   const int grid = static_cast<int>(std::min<size_t>(static_cast<size_t>(c.sm_count) * 16, (total + 255) / 256));

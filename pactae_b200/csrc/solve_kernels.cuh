@@ -652,13 +652,16 @@ __host__ __device__ constexpr int rank_layout() {
 // proposal then reads pref_m[m][r] and pr[m][r] side by side, sequentially,
 // instead of a random rankT[m][w] that waits for pref_m[m][r]; in congested
 // and correlated lists, where men reject hundreds of women per acceptance,
-// that halves the round trips of a window.  One CTA per man row at a time:
+// that halves the round trips of a window.  The same pass writes each man's
+// first K entries of the prefix table (woman << 16 | rank, as k_prefix
+// would).  One CTA per man row at a time:
 // his rankT row is staged in shared memory (16-byte loads over its aligned
 // interior), his pref_m row streams in with 16-byte loads and gathers from
 // it.  An out-of-range woman is reported.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(512) k_pr(const int32_t *__restrict__ pref_m, const uint16_t *__restrict__ rankT,
-                                            uint16_t *__restrict__ pr, int n, Control *ctrl, int gate) {
+                                            uint16_t *__restrict__ pr, uint32_t *__restrict__ prefix, int K, int n,
+                                            Control *ctrl, int gate) {
   if (!gate_open(gate, ctrl)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tid = threadIdx.x;
@@ -677,11 +680,14 @@ __global__ void __launch_bounds__(512) k_pr(const int32_t *__restrict__ pref_m, 
     __syncthreads();
     const RowSpan s = row_span(pref_m, m, n);
     uint16_t *out = pr + static_cast<size_t>(m) * n;
+    uint32_t *pfx = prefix + static_cast<size_t>(m) * K;  // his first K choices, packed as k_prefix does
     const auto gather = [&](int w, int r) {
       if (static_cast<unsigned>(w) < static_cast<unsigned>(n)) {
         out[r] = srow[w];
+        if (r < K) pfx[r] = (static_cast<uint32_t>(w) << 16) | srow[w];
       } else {
         bad = true;
+        if (r < K) pfx[r] = 0xFFFFFFFFu;
       }
     };
     if (tid < s.head) gather(__ldcs(s.row + tid), tid);
@@ -696,7 +702,7 @@ __global__ void __launch_bounds__(512) k_pr(const int32_t *__restrict__ pref_m, 
     for (int i = tid; i < s.nq; i += nthr) {
       const int4 q = __ldcs(s.rq + i);
       const int r = s.head + 4 * i;
-      if (wide) {
+      if (wide && r >= K) {  // no prefix entry among the four
         const uint2 v = make_uint2(rank_or_flag(q.x) | (rank_or_flag(q.y) << 16),
                                    rank_or_flag(q.z) | (rank_or_flag(q.w) << 16));
         *reinterpret_cast<uint2 *>(out + r) = v;
