@@ -258,6 +258,31 @@ def test_deep_chain_families_match_oracle(ctx, kind, n, param):
     assert st["blocking_pairs"] == 0
 
 
+@pytest.mark.parametrize("where", ["man_deep", "man_first_choices", "woman_row"])
+def test_rank_mode_rejects_bad_entries(ctx, where):
+    # Congested lists take the rank mode: inversion, transpose, ranks by
+    # position.  A bad entry anywhere must end the solve with the status, and
+    # the context must solve the intact instance afterwards.
+    n = 1001
+    pm, pw = oracle.generate(pb.SMP_GEN_CONGESTED, n, 5)
+    pm = pm.copy()
+    pw = pw.copy()
+    if where == "man_deep":
+        pm[7, 900] = n + 3
+    elif where == "man_first_choices":
+        pm[11, 3] = -2
+    else:
+        pw[20, 10] = pw[20, 11]
+    with pytest.raises(pb.SmpError) as e:
+        ctx.solve(pm, pw)
+    assert e.value.status == pb.SMP_ERR_INVALID_INPUT
+    pm2, pw2 = oracle.generate(pb.SMP_GEN_CONGESTED, n, 5)
+    match, st = ctx.solve(pm2, pw2)
+    want, props = oracle.gs_seq(pm2, pw2)
+    assert np.array_equal(match, want) and st["proposals"] == props
+    assert st["mode"] == 0
+
+
 def test_bad_arguments(ctx):
     with pytest.raises(pb.SmpError) as e:
         ctx.generate(pb.SMP_GEN_SOLO, 2, seed=1)
