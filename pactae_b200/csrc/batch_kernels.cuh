@@ -61,7 +61,7 @@ __device__ __forceinline__ void batch_scatter(uint16_t *srow, int m, int r, int 
 }
 
 __device__ __forceinline__ void batch_invert_slab(const int32_t *__restrict__ pref_w, uint16_t *slab, int n, int G,
-                                                  uint16_t *buf, bool &bad) {
+                                                  uint16_t *buf, bool &bad, bool store = true) {
   const int tid = threadIdx.x;
   const int nthr = blockDim.x;
   const int warp = tid >> 5;
@@ -107,7 +107,7 @@ __device__ __forceinline__ void batch_invert_slab(const int32_t *__restrict__ pr
       if (first >= 0 && first + 8 <= n) {
         bad |= (__vcmpeq2(v.x, 0xFFFFFFFFu) | __vcmpeq2(v.y, 0xFFFFFFFFu) | __vcmpeq2(v.z, 0xFFFFFFFFu) |
                 __vcmpeq2(v.w, 0xFFFFFFFFu)) != 0u;
-        reinterpret_cast<uint4 *>(out - pre)[c] = v;
+        if (store) reinterpret_cast<uint4 *>(out - pre)[c] = v;
       } else {
         const uint16_t *vals = reinterpret_cast<const uint16_t *>(&v);
 #pragma unroll
@@ -115,7 +115,7 @@ __device__ __forceinline__ void batch_invert_slab(const int32_t *__restrict__ pr
           const int e = first + k;
           if (e >= 0 && e < n) {
             bad |= vals[k] == 0xFFFFu;
-            out[e] = vals[k];
+            if (store) out[e] = vals[k];
           }
         }
       }
@@ -140,6 +140,7 @@ __global__ void __launch_bounds__(512, 2) k_batch(BatchInstance *__restrict__ ta
   __shared__ int s_status;
   __shared__ int s_bad;
   __shared__ unsigned long long s_props;
+  __shared__ int s_swap;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
@@ -165,13 +166,114 @@ __global__ void __launch_bounds__(512, 2) k_batch(BatchInstance *__restrict__ ta
     }
     uint16_t *const rank =
         static_cast<long long>(n) * n <= static_cast<long long>(rank_smem_elems) ? srank : slab;
-    for (int w = tid; w < n; w += blockDim.x) sbid[w] = 0xFFFFFFFFu;
     if (tid == 0) {
       s_next_man = 0;
       s_status = 0;
       s_bad = 0;
       s_props = 0;
+      s_swap = 2 * n <= rank_smem_elems && n >= 16;  // n >= 16: a row fits the bid words' memory
     }
+    __syncthreads();
+
+    // 0. Do all men share one list?  Then the stable matching is unique --
+    // woman pi_1 gets her favourite man, pi_2 her favourite of the rest, ...
+    // -- so the women-proposing run finds the same matching, with about
+    // n ln n proposals instead of the men's n (n + 1) / 2; and the men's
+    // proposal count is n (n + 1) / 2, each woman's place in the shared list
+    // counted once.  The first choices are screened first; the full
+    // comparison reads pref_m once.
+    volatile int *swap_flag = &s_swap;
+    if (*swap_flag) {
+      const int first = __ldg(pref_m);
+      for (int m = tid; m < n; m += blockDim.x)
+        if (__ldg(pref_m + static_cast<size_t>(m) * n) != first) *swap_flag = 0;
+    }
+    __syncthreads();
+    uint16_t *const inv = srank;      // inv[w] = her place in the shared list
+    uint16_t *const row0 = srank + n;  // the shared list
+    if (s_swap) {
+      for (int w = tid; w < n; w += blockDim.x) inv[w] = 0xFFFFu;
+      __syncthreads();
+      for (int r = tid; r < n; r += blockDim.x) {
+        const int w = __ldg(pref_m + r);
+        if (static_cast<unsigned>(w) < static_cast<unsigned>(n)) {
+          row0[r] = static_cast<uint16_t>(w);
+          inv[w] = static_cast<uint16_t>(r);
+        } else {
+          *swap_flag = 0;  // the ordinary path reports it
+        }
+      }
+      __syncthreads();
+      for (int w = tid; w < n; w += blockDim.x)
+        if (inv[w] == 0xFFFFu) *swap_flag = 0;  // not a permutation: the ordinary path reports it
+      for (int m = 1 + warp; m < n; m += nwarps) {
+        int go = 0;
+        if (lane == 0) go = *swap_flag;
+        if (!__shfl_sync(kFullMask, go, 0)) break;  // the whole warp leaves together
+        const int32_t *row = pref_m + static_cast<size_t>(m) * n;
+        bool same = true;
+        for (int r = lane; r < n; r += 32) same &= __ldg(row + r) == static_cast<int>(row0[r]);
+        if (!__all_sync(kFullMask, same) && lane == 0) *swap_flag = 0;
+      }
+      __syncthreads();
+    }
+    if (s_swap) {
+      // the women's lists must be permutations too: checked in groups of
+      // rows through the bid words' shared memory, which is free until now
+      bool bad = false;
+      const int G = min(static_cast<int>(batch_smem_bytes(max_n) / 2) / batch_row_slots(n), nwarps);
+      batch_invert_slab(pref_w, slab, n, G, reinterpret_cast<uint16_t *>(smem_raw), bad, false);
+      if (bad) s_status = SMP_ERR_INVALID_INPUT;
+      __syncthreads();
+      for (int m = tid; m < n; m += blockDim.x) sbid[m] = 0xFFFFFFFFu;  // the men, holding no woman
+      __syncthreads();
+      {
+        // women propose down their lists; every man ranks a woman by her
+        // place in the shared list
+        const SharedBids bids{sbid, spos};
+        const auto keep_going = [&]() { return *reinterpret_cast<volatile int *>(&s_status) == 0; };
+        int m = -1, pos = 0, S = 1, bad_value = 0;
+        Ahead ahead;
+        unsigned long long settled = 0;
+        unsigned int hops = 0;
+        while (keep_going()) {
+          if (m < 0) {
+            int i = 0;
+            if (lane == 0) i = atomicAdd(&s_next_man, 1);
+            i = __shfl_sync(kFullMask, i, 0);
+            if (i >= n) break;
+            m = i;
+            pos = 0;
+            S = 1;
+          }
+          const int rc = man_step<kMaxSub, true, false, 1, 3>(bids, keep_going, pref_w,
+                                                               static_cast<const uint16_t *>(inv),
+                                                               static_cast<const uint32_t *>(nullptr), 0, n, false,
+                                                               lane, m, pos, S, ahead, settled, hops, bad_value);
+          if (rc == kStepMoved || rc == kStepMatchedFree) continue;
+          if (rc == kStepBad && lane == 0) s_status = SMP_ERR_INVALID_INPUT;
+          break;
+        }
+      }
+      __syncthreads();
+      if (!s_status)
+        for (int m = tid; m < n; m += blockDim.x) {
+          const uint32_t b = sbid[m];
+          if (b == 0xFFFFFFFFu) {
+            s_bad = 1;
+            continue;
+          }
+          inst->match[m] = static_cast<int32_t>(b & 0xFFFFu);
+        }
+      __syncthreads();
+      if (tid == 0) {
+        inst->status = s_status ? s_status : (s_bad ? SMP_ERR_INVALID_INPUT : SMP_OK);
+        inst->proposals = s_status || s_bad ? 0ull : static_cast<unsigned long long>(n) * (n + 1) / 2;
+      }
+      __syncthreads();
+      continue;
+    }
+    for (int w = tid; w < n; w += blockDim.x) sbid[w] = 0xFFFFFFFFu;
     __syncthreads();
 
     // 1. inversion: through the shared region in groups of rows when the

@@ -36,7 +36,10 @@ __device__ __forceinline__ uint32_t issue_choice(const int32_t *__restrict__ pre
 //   1 (true)   man-major, rank[m][w], so a man's scan stays within his row;
 //   2          by position, pr[m][r] = the rank of man m in the list of his
 //              r-th choice: read at the index of his pref_m entry, so its
-//              load does not wait for that one.
+//              load does not wait for that one;
+//   3          one rank per proposer, rank[m]: every receiver ranks the
+//              proposers the same way (a batch instance solved with the
+//              roles swapped because all men share one list).
 template <bool kLdg = true, int kManMajor = 0, typename RankT>
 __device__ __forceinline__ int finish_choice(uint32_t raw, const RankT *__restrict__ rank, int K, int n, bool query,
                                              int m, int r, int &w, uint32_t &rk) {
@@ -49,7 +52,8 @@ __device__ __forceinline__ int finish_choice(uint32_t raw, const RankT *__restri
   if (query) return 1;
   w = static_cast<int>(raw);
   if (static_cast<unsigned>(w) >= static_cast<unsigned>(n)) return 2;
-  const RankT *p = kManMajor == 2   ? rank + static_cast<size_t>(m) * n + r
+  const RankT *p = kManMajor == 3   ? rank + m
+                   : kManMajor == 2 ? rank + static_cast<size_t>(m) * n + r
                    : kManMajor == 1 ? rank + static_cast<size_t>(m) * n + w
                                     : rank + static_cast<size_t>(w) * n + m;
   rk = static_cast<uint32_t>(kLdg ? __ldg(p) : *p);

@@ -74,6 +74,52 @@ def test_batch_flags_a_bad_instance_only(ctx):
     assert all(s == 0 for i, s in enumerate(status) if i != 4)
 
 
+def test_batch_men_sharing_one_list(ctx):
+    # All men share one list (the congested family): the batch solves these
+    # with the women proposing, as the stable matching is unique; matchings
+    # and the men's proposal counts must equal the oracle's.  Odd sizes, and
+    # near-congested instances (one man's list differs) that must not take
+    # that path.
+    import torch
+
+    insts, wants = [], []
+    for b, n in enumerate([16, 17, 333, 1001, 2048]):
+        pm, pw = oracle.generate(pb.SMP_GEN_CONGESTED, n, 40 + b)
+        for twist in (False, True):
+            pm2 = pm.copy()
+            if twist:  # one man swaps two choices: lists no longer shared
+                pm2[n // 2, [n - 2, n - 1]] = pm2[n // 2, [n - 1, n - 2]]
+            wants.append(oracle.gs_seq(pm2, pw))
+            insts.append((torch.from_numpy(pm2).cuda(), torch.from_numpy(pw).cuda(),
+                          torch.full((n,), -1, dtype=torch.int32, device="cuda")))
+    with pb.Batch(ctx, insts) as batch:
+        status, props, st = batch.run()
+    assert all(s == 0 for s in status)
+    for (_, _, mt), (want, wp), p in zip(insts, wants, props):
+        assert np.array_equal(mt.cpu().numpy(), want) and p == wp
+
+
+@pytest.mark.parametrize("where", ["woman_row", "shared_list"])
+def test_batch_men_sharing_one_list_bad_input(ctx, where):
+    import torch
+
+    n = 300
+    pm, pw = oracle.generate(pb.SMP_GEN_CONGESTED, n, 7)
+    pm, pw = pm.copy(), pw.copy()
+    if where == "woman_row":
+        pw[5, 3] = pw[5, 4]  # a woman's list is not a permutation
+    else:
+        pm[:, 10] = pm[:, 11]  # the shared list is not a permutation
+    good_pm, good_pw = oracle.generate(pb.SMP_GEN_CONGESTED, n, 8)
+    insts = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(),
+              torch.full((n,), -1, dtype=torch.int32, device="cuda")) for a, b in ((pm, pw), (good_pm, good_pw))]
+    with pb.Batch(ctx, insts) as batch:
+        status, props, st = batch.run()
+    assert status[0] == pb.SMP_ERR_INVALID_INPUT and status[1] == 0
+    want, wp = oracle.gs_seq(good_pm, good_pw)
+    assert np.array_equal(insts[1][2].cpu().numpy(), want) and props[1] == wp
+
+
 # -- shapes: the rank matrix on chip or in the slab, tuned or fixed ------------
 @pytest.mark.parametrize("rank_smem_kb", [-1, 32, 96])
 def test_shared_and_global_rank_agree(ctx, rank_smem_kb):
