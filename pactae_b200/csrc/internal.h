@@ -120,6 +120,10 @@ struct Ctx {
   bool rank_valid = false;  // d_rank holds the inversion of pref_w
   bool tail_ran = false;
   int phase = 0;            // 0 staged, 1 prechecked, 2 inited, 3 cored, 4 posted
+  // The mode the host has read back from the precheck (kModeQuery / kModeRank),
+  // or -1: the enqueue functions then skip the kernels that mode would gate
+  // off.  -1 (unknown) enqueues everything and the device picks.
+  int known_mode = -1;
 
   DeviceBuf d_pref_m, d_pref_w, d_rank, d_rankT, d_pr, d_prefix, d_bid, d_tailq, d_seen, d_ctrl, d_match;
   DeviceBuf d_husband, d_prank;

@@ -300,14 +300,14 @@ int init_buffers(Ctx &c) {
 int enqueue_init(Ctx &c) {
   int rc = init_buffers(c);
   if (rc) return rc;
-  if (c.query_ok) {
+  if (c.query_ok && c.known_mode != kModeRank) {
     rc = enqueue_query(c);
     if (rc) return rc;
   }
-  rc = enqueue_rank(c, kGateModeRank);
+  if (c.known_mode != kModeQuery) rc = enqueue_rank(c, kGateModeRank);
   if (rc) return rc;
   if (cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
-  return enqueue_prefix_gather(c, kGateModeRank);
+  return c.known_mode == kModeQuery ? SMP_OK : enqueue_prefix_gather(c, kGateModeRank);
 }
 
 template <typename RankT, int kSub>
@@ -316,7 +316,7 @@ int launch_bulk(Ctx &c, int round) {
   const uint32_t *prefix = c.K > 0 ? c.d_prefix.as<uint32_t>() : nullptr;
   const int rank_threshold = c.tail_threshold > 0 ? std::min(c.tail_threshold, c.tail_threshold_rank) : 0;
   const size_t filter = sizeof(uint32_t) * static_cast<size_t>(c.n);
-  if (round == 0 && filter + 1024 <= c.smem_optin) {  // the shared partner-rank filter fits
+  if (round == 0 && c.known_mode != kModeQuery && filter + 1024 <= c.smem_optin) {  // the filter fits
     // k_wdistinct decides on the device which of the two variants runs
     k_wdistinct<<<1, 1024, sizeof(uint32_t) * ((c.n + 31) / 32), c.stream>>>(c.pref_w, c.n, c.d_ctrl.as<Control>());
     c.launches++;
@@ -333,14 +333,14 @@ int launch_bulk(Ctx &c, int round) {
     }
     kernel<<<c.sm_count * std::max(per_sm, 1), kFilterBlock, filter, c.stream>>>(
         c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(), c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
-        c.n, c.tail_threshold, rank_threshold, round);
+        c.n, c.tail_threshold, rank_threshold, round, -1);
     c.launches++;
     rc = c.check_launch("k_bulk (filtered)");
     if (rc) return rc;
   }
   k_bulk<RankT, kSub><<<resident_grid(c, k_bulk<RankT, kSub>, 256), 256, 0, c.stream>>>(
       c.pref_m, rank, prefix, c.K, c.d_bid.as<unsigned long long>(), c.d_ctrl.as<Control>(), c.d_tailq.as<int2>(),
-      c.n, c.tail_threshold, rank_threshold, round);
+      c.n, c.tail_threshold, rank_threshold, round, c.known_mode);
   c.launches++;
   return c.check_launch("k_bulk");
 }
@@ -403,8 +403,8 @@ int enqueue_round(Ctx &c, int round) {
   // Query-mode instances end in short chains, every choice in the prefix
   // (k_tail_q); rank-mode ones in deep scans (wide look-ahead).  Both are
   // enqueued and the device runs the one for the mode the precheck chose.
-  rc = launch_tail_query(c);
-  if (!rc) rc = launch_tail_window<RankT>(c, kRankTailWindow, round, kModeRank);
+  if (c.known_mode != kModeRank) rc = launch_tail_query(c);
+  if (!rc && c.known_mode != kModeQuery) rc = launch_tail_window<RankT>(c, kRankTailWindow, round, kModeRank);
   return rc;
 }
 
@@ -429,7 +429,8 @@ int enqueue_core_t(Ctx &c) {
   if (rc) return rc;
   c.tail_ran = c.tail_threshold > 0;
   rc = enqueue_round<RankT>(c, 0);
-  if (rc || !c.query_ok) return rc;
+  // with the mode known, the caller enqueues the retry round if round 0 asks
+  if (rc || !c.query_ok || c.known_mode >= 0) return rc;
   return enqueue_retry_round<RankT>(c);
 }
 
@@ -506,6 +507,7 @@ int stage_reset(Ctx &c, int32_t n) {
   c.stats.n = n;
   c.stats.blocking_pairs = -1;
   c.launches = 0;
+  c.known_mode = -1;
   plan(c);
   return SMP_OK;
 }
@@ -657,6 +659,75 @@ int solve_enqueue(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t 
   return rc;
 }
 
+// The synchronous solve, in one pass when the precheck picks the query mode
+// (uniform-like inputs): the pass enqueues only that mode's kernels -- the
+// bulk restricted to it, so a rank-mode instance cannot start proposing
+// before its ranks exist -- through the match copy, and the host waits once.
+// If the precheck chose the rank mode, or a man went beyond his prefix, a
+// second pass enqueues what remains and copies the match again.  Kernels a
+// mode gates off would still cost a launch and a pass of every CTA over the
+// gate: 14 of them took about 0.1 ms of a 2.6 ms uniform solve at
+// n = 30000, where a wait for the precheck costs about 30 us.  The kernels
+// keep their gates, so the device still decides what runs.  The checker
+// (SMP_F_CHECK) must see the final matching: those solves take the fully
+// gated pipeline.
+int solve_staged(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
+                 uint32_t flags, smp_stats *st) {
+  // the checker, a disabled tail or a configured tail window (whose tail
+  // kernel serves either mode) take the fully gated pipeline
+  if ((flags & SMP_F_CHECK) || !(c.tail_threshold > 0) || c.tail_window_cfg > 0) {
+    int rc = solve_enqueue(c, pref_m, pref_w, n, match_out, flags);
+    if (!rc) rc = c.sync("solve");
+    return rc ? rc : solve_finish(c, flags, st);
+  }
+  int rc = do_stage(c, pref_m, pref_w, n, flags);
+  if (rc) return rc;
+  const auto finish_pass = [&]() {
+    int r = SMP_OK;
+    if (cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) r = c.fail_cuda("event");
+    if (!r) r = enqueue_post(c);
+    if (!r && (flags & SMP_F_DEVICE_PTRS)) r = copy_match_out(c, match_out, true);
+    if (!r && cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) r = c.fail_cuda("event");
+    if (!r && !(flags & SMP_F_DEVICE_PTRS)) r = copy_match_out(c, match_out, false);
+    if (!r) r = read_control(c);
+    if (!r) r = c.sync("solve");
+    return r;
+  };
+  // pass 1: as if the precheck picks the query mode
+  rc = enqueue_precheck(c, (flags & SMP_F_NO_PRECHECK) == 0);
+  if (!rc && (flags & SMP_F_VALIDATE)) rc = enqueue_validate(c);
+  if (!rc && cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  const bool speculate = c.query_ok;
+  if (speculate) {
+    c.known_mode = kModeQuery;
+    if (!rc) rc = enqueue_init(c);
+    if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    if (!rc) rc = enqueue_core(c);
+    if (!rc) rc = finish_pass();
+  } else {
+    if (!rc) rc = read_control(c);
+    if (!rc) rc = c.sync("precheck");
+  }
+  if (rc) return rc;
+  const Control &h = *c.h_ctrl;
+  const bool done = speculate && !h.status && (h.perfect || (h.mode == kModeQuery && !h.retry));
+  if (!done && !h.status) {
+    // pass 2: the rank mode, or the rank-mode retry of a query-mode round 0
+    if (speculate && h.mode == kModeQuery && h.retry) {
+      c.known_mode = -1;
+      rc = c.rank_bytes == 2 ? enqueue_retry_round<uint16_t>(c) : enqueue_retry_round<int32_t>(c);
+    } else {
+      c.known_mode = h.perfect ? -1 : h.mode;
+      rc = enqueue_init(c);
+      if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+      if (!rc) rc = enqueue_core(c);
+    }
+    if (!rc) rc = finish_pass();
+    if (rc) return rc;
+  }
+  return solve_finish(c, flags, st);
+}
+
 // Statistics and status of a solve whose stream has completed.
 int solve_finish(Ctx &c, uint32_t flags, smp_stats *st) {
   c.phase = 3;
@@ -726,6 +797,7 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
                : c.fail_cuda("pref_m copy");
   };
   const bool query = c.h_ctrl->mode == kModeQuery && !c.h_ctrl->perfect;
+  if (!c.h_ctrl->perfect) c.known_mode = c.h_ctrl->mode;  // enqueue only this mode's kernels
   if (!query) {
     if (!c.h_ctrl->perfect) {
       rc = copy_rest_of_m();
@@ -761,6 +833,7 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
     if (!rc) rc = read_control(c);
     if (!rc) rc = c.sync("round 0");
     if (!rc && c.h_ctrl->retry && !c.h_ctrl->status) {
+      c.known_mode = -1;
       rc = copy_rest_of_m();
       if (!rc) rc = enqueue_retry_round<uint16_t>(c);
     }
@@ -985,10 +1058,7 @@ int smp_b200_solve(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w, i
       return rc ? rc : smpb200::solve_streamed(c, pref_m, pref_w, n, match_out, flags, st);
     }
   }
-  int rc = smpb200::solve_enqueue(c, pref_m, pref_w, n, match_out, flags);
-  if (!rc) rc = c.sync("solve");
-  if (rc) return rc;
-  return smpb200::solve_finish(c, flags, st);
+  return smpb200::solve_staged(c, pref_m, pref_w, n, match_out, flags, st);
 }
 
 int smp_b200_invert(smp_ctx *ctx, const int32_t *pref_w, int32_t n, int32_t *rank_out, uint32_t flags) {

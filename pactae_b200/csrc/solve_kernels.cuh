@@ -774,7 +774,7 @@ template <typename RankT, int kMaxSub, bool kFilter = false>
 __global__ void __launch_bounds__(kFilter ? kFilterBlock : 256)
     k_bulk(const int32_t *__restrict__ pref_m, const RankT *__restrict__ rank, const uint32_t *__restrict__ prefix,
            int K, unsigned long long *bid, Control *ctrl, int2 *tail_queue, int n, int tail_threshold_query,
-           int tail_threshold_rank, int round) {
+           int tail_threshold_rank, int round, int only_mode = -1) {
   using Bids = typename std::conditional<kFilter, FilteredBids, GlobalBids>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint32_t *lrank = reinterpret_cast<uint32_t *>(smem_raw);
@@ -794,6 +794,8 @@ __global__ void __launch_bounds__(kFilter ? kFilterBlock : 256)
     if (!gate_open(round == 0 ? kGateMain : kGateRetry, ctrl)) return;
     if (round == 0 && ld_volatile_s32(&ctrl->retry)) return;  // a query bucket overflowed
     if (round == 0 && ld_volatile_s32(&ctrl->use_filter)) return;  // the filtered variant runs
+    // enqueued for one mode only (the host has not read the precheck yet)
+    if (round == 0 && only_mode >= 0 && ld_volatile_s32(&ctrl->mode) != only_mode) return;
   }
   const bool query = round == 0 && ld_volatile_s32(&ctrl->mode) == kModeQuery;
   // Free women left when the men move to the one-CTA tail: rank-mode
