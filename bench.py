@@ -286,10 +286,14 @@ def run_b200(args, dist: Dist) -> dict | None:
             e2e_times.append((time.perf_counter() - t0) * 1e3)
         e2e_total = dist.max(sum(e2e_times))
         assert np.array_equal(hm, match.cpu().numpy()), "e2e matching differs from the device-input solve"
-        # A host-input query-mode solve copies each man's first K choices and
-        # all of pref_w (streamed in row chunks under the inversion); rank
-        # mode and the retry copy both lists whole.
-        h2d = (4 * n * n + 4 * n * 192) if e2e_st["mode"] == 1 else 8 * n * n
+        # A host-input query-mode solve copies each man's first K = 192
+        # choices and all of pref_w, streamed in row chunks under the
+        # inversion -- packed to 16 bits on the host when n <= 32767; rank
+        # mode and the retry copy both lists whole as int32.
+        if e2e_st["mode"] == 1:
+            h2d = (2 if n <= 32767 else 4) * n * n + 4 * n * 192
+        else:
+            h2d = 8 * n * n
         e2e = {"value": e2e_total / (args.steps * dist.world), "unit": "ms",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": n * 4,
                "per_rank_ms_per_solve": e2e_total / args.steps,

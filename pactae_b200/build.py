@@ -32,7 +32,7 @@ NVCC_FLAGS = [
     "-Xptxas", "-warn-spills",
 ]
 
-SOURCES = ["smp_b200.cu", "generate.cu", "batch.cu", "serve.cu", "static_solve.cu", "workload_io.cpp"]
+SOURCES = ["smp_b200.cu", "generate.cu", "batch.cu", "serve.cu", "static_solve.cu", "workload_io.cpp", "host_pack.cpp"]
 
 
 def _nvcc() -> str:

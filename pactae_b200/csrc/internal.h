@@ -5,8 +5,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <cstdint>
+#include <functional>
+#include <memory>
 #include <mutex>
+#include <thread>
+#include <vector>
 #include <set>
 #include <utility>
 #include <array>
@@ -90,6 +95,62 @@ struct DeviceGuard {
   }
 };
 
+// A fixed set of host threads that run one job at a time: run(f) calls
+// f(i, count) on every worker i and returns when all have finished.  Started
+// once per context, so a call costs a wake-up, not a thread creation.
+// Entries [begin, end) of src packed to uint16 in dst (host_pack.cpp).
+void pack_u16(const int32_t *src, uint16_t *dst, size_t begin, size_t end, int n);
+
+class HostPool {
+ public:
+  explicit HostPool(int count) {
+    for (int i = 0; i < count; ++i) threads_.emplace_back([this, i] { work(i); });
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : threads_) t.join();
+  }
+  int size() const { return static_cast<int>(threads_.size()); }
+  void run(const std::function<void(int, int)> &f) {
+    std::unique_lock<std::mutex> lock(mu_);
+    job_ = &f;
+    pending_ = size();
+    ++generation_;
+    cv_.notify_all();
+    done_.wait(lock, [this] { return pending_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  void work(int i) {
+    unsigned seen = 0;
+    for (;;) {
+      const std::function<void(int, int)> *f;
+      {
+        std::unique_lock<std::mutex> lock(mu_);
+        cv_.wait(lock, [&] { return stop_ || generation_ != seen; });
+        if (stop_) return;
+        seen = generation_;
+        f = job_;
+      }
+      (*f)(i, size());
+      std::lock_guard<std::mutex> lock(mu_);
+      if (--pending_ == 0) done_.notify_all();
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_;
+  const std::function<void(int, int)> *job_ = nullptr;
+  unsigned generation_ = 0;
+  int pending_ = 0;
+  bool stop_ = false;
+};
+
 struct Control;  // common.cuh
 
 struct Ctx {
@@ -126,6 +187,12 @@ struct Ctx {
   int known_mode = -1;
 
   DeviceBuf d_pref_m, d_pref_w, d_rank, d_rankT, d_pr, d_prefix, d_bid, d_tailq, d_seen, d_ctrl, d_match;
+  DeviceBuf d_pw16;  // pref_w packed to uint16 (host-input solves)
+  // Host-input solves: two pinned buffers a chunk of pref_w is packed into
+  // while the other one is copied, and the threads that pack.
+  uint16_t *h_stage[2] = {nullptr, nullptr};
+  size_t h_stage_elems = 0;
+  std::unique_ptr<HostPool> pack_pool;
   DeviceBuf d_husband, d_prank;
   DeviceBuf d_qcnt, d_qlist;
   DeviceBuf gen_keys_a, gen_keys_b, gen_seg, gen_temp, gen_aux;
@@ -136,8 +203,8 @@ struct Ctx {
   static constexpr int kCopyChunks = 16;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_chunk[kCopyChunks] = {};
-  std::array<DeviceBuf *, 20> buffers() {
-    return {&d_pref_m, &d_pref_w, &d_rank,    &d_rankT,    &d_pr,     &d_prefix, &d_bid,    &d_tailq,
+  std::array<DeviceBuf *, 21> buffers() {
+    return {&d_pref_m, &d_pref_w, &d_pw16, &d_rank,    &d_rankT,    &d_pr,     &d_prefix, &d_bid,    &d_tailq,
             &d_seen,   &d_ctrl,   &d_match,   &d_husband,  &d_prank,  &d_qcnt,   &d_qlist,
             &gen_keys_a, &gen_keys_b, &gen_seg, &gen_temp, &gen_aux};
   }

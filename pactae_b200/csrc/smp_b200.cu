@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <type_traits>
 
 #include "common.cuh"
@@ -274,6 +275,23 @@ int enqueue_qinvert(Ctx &c, int w0, int w1) {
                                          w0, w1);
   c.launches++;
   return c.check_launch(c.n <= kColorMaxN ? "k_qinvert_c" : "k_qinvert");
+}
+
+// Rows [w0, w1) of pref_w packed to uint16 in d_pw16 (host-input solves).
+int enqueue_qinvert16(Ctx &c, int w0, int w1) {
+  const size_t smem = row_smem_bytes<uint16_t>(c.n);
+  if (allow_dynamic_smem(c, k_qinvert_p16) != cudaSuccess) return c.fail_cuda("k_qinvert_p16 smem attribute");
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_qinvert_p16, 256, smem) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const int qgrid = std::max(1, std::min(w1 - w0, c.sm_count * std::max(per_sm, 1)));
+  k_qinvert_p16<<<qgrid, 256, smem, c.stream>>>(c.d_pw16.as<uint16_t>(), c.n, c.K, query_capacity(c.n, c.K),
+                                                c.d_qcnt.as<int32_t>(), c.d_qlist.as<uint32_t>(),
+                                                c.d_prefix.as<uint32_t>(), c.d_ctrl.as<Control>(), w0, w1);
+  c.launches++;
+  return c.check_launch("k_qinvert_p16");
 }
 
 int enqueue_query(Ctx &c) {
@@ -760,6 +778,49 @@ bool streamed_fits(const Ctx &c, uint32_t flags) {
          c.tail_threshold > 0 && c.n >= kStreamMinN;
 }
 
+// Host-input query solves stream pref_w packed to uint16 -- half the bytes
+// on the host link, which is what an n = 30000 host-input solve waits for --
+// when the colour-tagged inversion applies (n <= kColorMaxN) and the host
+// has threads to pack with.  Sets up the pinned staging pair and the packing
+// threads on first use; false if packing does not apply.
+bool pack_ready(Ctx &c) {
+  const int n = c.n;
+  if (n > kColorMaxN || n < 8) return false;
+  const unsigned hw = std::thread::hardware_concurrency();
+  if (hw < 4) return false;
+  const size_t chunk = static_cast<size_t>((n + Ctx::kCopyChunks - 1) / Ctx::kCopyChunks + 1) * n;
+  if (c.h_stage_elems < chunk) {
+    for (auto &h : c.h_stage) {
+      if (h) cudaFreeHost(h);
+      h = nullptr;
+    }
+    c.h_stage_elems = 0;
+    for (auto &h : c.h_stage) {
+      if (cudaMallocHost(reinterpret_cast<void **>(&h), sizeof(uint16_t) * chunk) != cudaSuccess) {
+        cudaGetLastError();
+        for (auto &g : c.h_stage) {
+          if (g) cudaFreeHost(g);
+          g = nullptr;
+        }
+        return false;
+      }
+    }
+    c.h_stage_elems = chunk;
+  }
+  if (c.d_pw16.ensure(sizeof(uint16_t) * static_cast<size_t>(n) * n)) return false;
+  // eight packing threads: on a 16-core host with the copy engine reading
+  // the staging at the same time, sixteen packed no faster
+  if (!c.pack_pool) c.pack_pool.reset(new (std::nothrow) HostPool(static_cast<int>(std::min(hw, 8u))));
+  return c.pack_pool != nullptr;
+}
+
+// count entries of src into uint16 dst on the packing threads; an entry
+// outside [0, n) becomes a value >= n, which the inversion reports.
+void pack_rows(Ctx &c, const int32_t *src, uint16_t *dst, size_t count, int n) {
+  const auto job = [&](int i, int parts) { pack_u16(src, dst, count * i / parts, count * (i + 1) / parts, n); };
+  c.pack_pool->run(job);
+}
+
 int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
                    uint32_t flags, smp_stats *st) {
   const size_t row = sizeof(int32_t) * static_cast<size_t>(n);
@@ -812,19 +873,32 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
     if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
     rc = init_buffers(c);
     if (!rc) rc = enqueue_query_index(c);
+    const bool packed = !rc && pack_ready(c);
     for (int k = 0; !rc && k < Ctx::kCopyChunks; ++k) {
       const int r0 = static_cast<int>(static_cast<int64_t>(n) * k / Ctx::kCopyChunks);
       const int r1 = static_cast<int>(static_cast<int64_t>(n) * (k + 1) / Ctx::kCopyChunks);
       if (r0 == r1) continue;
       const size_t off = static_cast<size_t>(r0) * n;
-      if (cudaMemcpyAsync(dw + off, pref_w + off, row * (r1 - r0), cudaMemcpyHostToDevice, c.copy_stream) !=
-              cudaSuccess ||
-          cudaEventRecord(c.ev_chunk[k], c.copy_stream) != cudaSuccess ||
+      cudaError_t e;
+      if (packed) {
+        // the staging buffer this chunk uses was last copied two chunks ago
+        uint16_t *stage = c.h_stage[k & 1];
+        if (k >= 2 && cudaEventSynchronize(c.ev_chunk[k - 2]) != cudaSuccess) {
+          rc = c.fail_cuda("staging wait");
+          break;
+        }
+        pack_rows(c, pref_w + off, stage, static_cast<size_t>(r1 - r0) * n, n);
+        e = cudaMemcpyAsync(c.d_pw16.as<uint16_t>() + off, stage, sizeof(uint16_t) * static_cast<size_t>(r1 - r0) * n,
+                            cudaMemcpyHostToDevice, c.copy_stream);
+      } else {
+        e = cudaMemcpyAsync(dw + off, pref_w + off, row * (r1 - r0), cudaMemcpyHostToDevice, c.copy_stream);
+      }
+      if (e != cudaSuccess || cudaEventRecord(c.ev_chunk[k], c.copy_stream) != cudaSuccess ||
           cudaStreamWaitEvent(c.stream, c.ev_chunk[k], 0) != cudaSuccess) {
         rc = c.fail_cuda("pref_w chunk copy");
         break;
       }
-      rc = enqueue_qinvert(c, r0, r1);
+      rc = packed ? enqueue_qinvert16(c, r0, r1) : enqueue_qinvert(c, r0, r1);
     }
     if (!rc && cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
     if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
@@ -835,6 +909,9 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
     if (!rc && c.h_ctrl->retry && !c.h_ctrl->status) {
       c.known_mode = -1;
       rc = copy_rest_of_m();
+      // the rank-mode retry inverts pref_w itself: the packed copy will not do
+      if (!rc && packed && cudaMemcpyAsync(dw, pref_w, row * n, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+        rc = c.fail_cuda("pref_w copy");
       if (!rc) rc = enqueue_retry_round<uint16_t>(c);
     }
   }
@@ -944,6 +1021,9 @@ void smp_b200_destroy(smp_ctx *ctx) {
       if (e) cudaEventDestroy(e);
     if (c.copy_stream) cudaStreamDestroy(c.copy_stream);
     if (c.h_ctrl) cudaFreeHost(c.h_ctrl);
+    for (auto &h : c.h_stage)
+      if (h) cudaFreeHost(h);
+    c.pack_pool.reset();
     if (c.stream) cudaStreamDestroy(c.stream);
   }
   delete ctx;

@@ -719,6 +719,112 @@ __global__ void __launch_bounds__(512) k_pr(const int32_t *__restrict__ pref_m, 
   if (bad) report(ctrl, kStatusInvalidInput, -1);
 }
 
+// The same inversion from rows packed to uint16 on the host (host-input
+// solves stream pref_w in half the bytes): 16-byte loads hold 8 entries, and
+// a row starts anywhere on a 2-byte boundary, so up to 7 entries before its
+// first 16-byte boundary and 7 after its last are loaded one by one.
+struct RowSpan16 {
+  const uint16_t *row;
+  const uint4 *rq;  // first 16-byte aligned entry
+  int head, nq, tail;
+};
+
+__device__ __forceinline__ RowSpan16 row_span16(const uint16_t *pref16, int w, int n) {
+  RowSpan16 s;
+  s.row = pref16 + static_cast<size_t>(w) * n;
+  s.head = min(n, static_cast<int>(((16u - (reinterpret_cast<uintptr_t>(s.row) & 15u)) & 15u) >> 1));
+  s.rq = reinterpret_cast<const uint4 *>(s.row + s.head);
+  s.nq = (n - s.head) >> 3;
+  s.tail = n - s.head - 8 * s.nq;
+  return s;
+}
+
+__global__ void __launch_bounds__(256) k_qinvert_p16(const uint16_t *__restrict__ pref16, int n, int K, int qcap,
+                                                     const int32_t *__restrict__ qcnt,
+                                                     const uint32_t *__restrict__ qlist,
+                                                     uint32_t *__restrict__ prefix, Control *ctrl, int w0, int w1) {
+  if (!gate_open(kGateModeQuery, ctrl) || ld_volatile_s32(&ctrl->retry)) return;
+  int w = w0 + static_cast<int>(blockIdx.x);
+  if (w >= w1) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint16_t *srow = reinterpret_cast<uint16_t *>(smem_raw);
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;
+  const int chunks = (n + 7) / 8;
+  uint4 *s4 = reinterpret_cast<uint4 *>(srow);
+  for (int c = tid; c < chunks; c += nthr) s4[c] = make_uint4(~0u, ~0u, ~0u, ~0u);
+  bool bad = false;
+  RowSpan16 s = row_span16(pref16, w, n);
+  const auto load = [&](const RowSpan16 &sp, int base, uint4 (&v)[2]) {
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int i = base + tid + j * nthr;
+      v[j] = i < sp.nq ? __ldcs(sp.rq + i) : make_uint4(0, 0, 0, 0);
+    }
+  };
+  const auto scatter8 = [&](uint4 v, int r, uint32_t cbit) {
+    const uint32_t q[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      scatter_c(srow, static_cast<int>(q[h] & 0xFFFFu), r + 2 * h, cbit, n, bad);
+      scatter_c(srow, static_cast<int>(q[h] >> 16), r + 2 * h + 1, cbit, n, bad);
+    }
+  };
+  uint4 a[2];
+  load(s, 0, a);
+  int edge = tid < s.head ? __ldcs(s.row + tid) : (tid < s.head + s.tail ? __ldcs(s.row + s.head + 8 * s.nq + (tid - s.head)) : 0);
+  __syncthreads();  // the fill before the first scatter
+  for (int k = 0;; ++k) {
+    const uint32_t cbit = static_cast<uint32_t>(k & 1) << 15;
+    if (tid < s.head) scatter_c(srow, edge, tid, cbit, n, bad);
+    else if (tid < s.head + s.tail) scatter_c(srow, edge, s.head + 8 * s.nq + (tid - s.head), cbit, n, bad);
+    for (int base = 0; base < s.nq; base += 2 * nthr) {
+      if (base > 0) load(s, base, a);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int i = base + tid + j * nthr;
+        if (i < s.nq) scatter8(a[j], s.head + 8 * i, cbit);
+      }
+    }
+    __syncthreads();  // row w complete in shared memory
+    const int wn = w + static_cast<int>(gridDim.x);
+    const RowSpan16 sn = row_span16(pref16, wn < w1 ? wn : w, n);
+    if (wn < w1) {
+      load(sn, 0, a);
+      edge = tid < sn.head ? __ldcs(sn.row + tid)
+                           : (tid < sn.head + sn.tail ? __ldcs(sn.row + sn.head + 8 * sn.nq + (tid - sn.head)) : 0);
+    }
+    const uint32_t want = cbit ? 0x80008000u : 0u;
+    for (int c = tid; c < chunks; c += nthr) {
+      const uint4 v = s4[c];
+      const int tailn = n - c * 8;
+      uint32_t m0 = 0x80008000u, m1 = 0x80008000u, m2 = 0x80008000u, m3 = 0x80008000u;
+      if (tailn < 8) {
+        const auto keep = [tailn](int half) -> uint32_t {
+          return (half < tailn ? 0x00008000u : 0u) | (half + 1 < tailn ? 0x80000000u : 0u);
+        };
+        m0 = keep(0);
+        m1 = keep(2);
+        m2 = keep(4);
+        m3 = keep(6);
+      }
+      bad |= (((v.x ^ want) & m0) | ((v.y ^ want) & m1) | ((v.z ^ want) & m2) | ((v.w ^ want) & m3)) != 0u;
+    }
+    const uint32_t *bucket = qlist + static_cast<size_t>(w) * qcap;
+    const int count = min(__ldg(qcnt + w), qcap);
+    for (int q = tid; q < count; q += nthr) {
+      const uint32_t e = bucket[q];
+      const uint32_t m = e >> 16, r = e & 0xFFFFu;
+      prefix[static_cast<size_t>(m) * K + r] = (static_cast<uint32_t>(w) << 16) | (srow[m] & 0x7FFFu);
+    }
+    __syncthreads();  // answers read before the next row overwrites
+    if (wn >= w1) break;
+    w = wn;
+    s = sn;
+  }
+  if (bad) report(ctrl, kStatusInvalidInput, -1);
+}
+
 // ---------------------------------------------------------------------------
 // Bulk proposals on every SM.  Each warp carries one free man at a time
 // (man_step above, 64-bit bids in HBM).  A man accepted by a free woman

@@ -214,18 +214,24 @@ def test_invalid_inputs_rejected(ctx):
 
 
 @pytest.mark.parametrize("n,row", [(4999, 10), (4999, 4990), (6000, 3001)])
-@pytest.mark.parametrize("defect", ["duplicate", "out_of_range"])
+@pytest.mark.parametrize("defect", ["duplicate", "out_of_range", "negative", "wraps_to_valid"])
 @pytest.mark.parametrize("host", [False, True])
 def test_bad_row_deep_in_the_inversion(ctx, n, row, defect, host):
     # At these sizes each CTA of the query-mode inversion works through many
     # rows, so a bad row is found after rows that were permutations (row 10
-    # is the first row of its CTA).  Host inputs take the streamed path.
+    # is the first row of its CTA).  Host inputs take the streamed path,
+    # which packs pref_w to 16 bits on the host: a -1 where the 0 was, or
+    # v + 65536 where v was, must not pack into a permutation.
     pm, pw = ctx.generate(pb.SMP_GEN_UNIFORM, n, seed=77)
     pw = pw.clone()
     if defect == "duplicate":
         pw[row, 5] = pw[row, 6]
-    else:
+    elif defect == "out_of_range":
         pw[row, n - 1] = n + 5
+    elif defect == "negative":
+        pw[row, int((pw[row] == 0).nonzero()[0, 0])] = -1
+    else:
+        pw[row, 7] += 65536
     if host:
         pm, pw = to_host(pm), to_host(pw)
     with pytest.raises(pb.SmpError) as e:
