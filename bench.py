@@ -287,11 +287,13 @@ def run_b200(args, dist: Dist) -> dict | None:
         e2e_total = dist.max(sum(e2e_times))
         assert np.array_equal(hm, match.cpu().numpy()), "e2e matching differs from the device-input solve"
         # A host-input query-mode solve copies each man's first K = 192
-        # choices and all of pref_w, streamed in row chunks under the
-        # inversion -- packed to 16 bits on the host when n <= 32767; rank
-        # mode and the retry copy both lists whole as int32.
+        # choices and all of pref_w, streamed in 16 row chunks under the
+        # inversion -- when n <= 32767 packed to 16 bits on the host except
+        # chunks 4 and 12, which cross as int32; rank mode and the retry copy
+        # both lists whole as int32.
         if e2e_st["mode"] == 1:
-            h2d = (2 if n <= 32767 else 4) * n * n + 4 * n * 192
+            rows = [n * (k + 1) // 16 - n * k // 16 for k in range(16)]
+            h2d = 4 * n * 192 + sum(r * n * (4 if n > 32767 or k % 8 == 4 else 2) for k, r in enumerate(rows))
         else:
             h2d = 8 * n * n
         e2e = {"value": e2e_total / (args.steps * dist.world), "unit": "ms",

@@ -188,9 +188,10 @@ struct Ctx {
 
   DeviceBuf d_pref_m, d_pref_w, d_rank, d_rankT, d_pr, d_prefix, d_bid, d_tailq, d_seen, d_ctrl, d_match;
   DeviceBuf d_pw16;  // pref_w packed to uint16 (host-input solves)
-  // Host-input solves: two pinned buffers a chunk of pref_w is packed into
-  // while the other one is copied, and the threads that pack.
-  uint16_t *h_stage[2] = {nullptr, nullptr};
+  // Host-input solves: a ring of pinned buffers the chunks of pref_w are
+  // packed into while earlier ones are copied, and the threads that pack.
+  static constexpr int kStageDepth = 3;
+  uint16_t *h_stage[kStageDepth] = {};
   size_t h_stage_elems = 0;
   std::unique_ptr<HostPool> pack_pool;
   DeviceBuf d_husband, d_prank;

@@ -781,7 +781,7 @@ bool streamed_fits(const Ctx &c, uint32_t flags) {
 // Host-input query solves stream pref_w packed to uint16 -- half the bytes
 // on the host link, which is what an n = 30000 host-input solve waits for --
 // when the colour-tagged inversion applies (n <= kColorMaxN) and the host
-// has threads to pack with.  Sets up the pinned staging pair and the packing
+// has threads to pack with.  Sets up the pinned staging ring and the packing
 // threads on first use; false if packing does not apply.
 bool pack_ready(Ctx &c) {
   const int n = c.n;
@@ -808,9 +808,9 @@ bool pack_ready(Ctx &c) {
     c.h_stage_elems = chunk;
   }
   if (c.d_pw16.ensure(sizeof(uint16_t) * static_cast<size_t>(n) * n)) return false;
-  // eight packing threads: on a 16-core host with the copy engine reading
-  // the staging at the same time, sixteen packed no faster
-  if (!c.pack_pool) c.pack_pool.reset(new (std::nothrow) HostPool(static_cast<int>(std::min(hw, 8u))));
+  // twelve packing threads: on a 16-core host with the copy engine reading
+  // the staging at the same time, eight were slower and sixteen no faster
+  if (!c.pack_pool) c.pack_pool.reset(new (std::nothrow) HostPool(static_cast<int>(std::min(hw, 12u))));
   return c.pack_pool != nullptr;
 }
 
@@ -874,19 +874,28 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
     rc = init_buffers(c);
     if (!rc) rc = enqueue_query_index(c);
     const bool packed = !rc && pack_ready(c);
+    // Packed chunks go through the staging ring; chunks 4 and 12 of 16 cross
+    // as int32 straight from the caller's buffer, keeping the link busy
+    // while the packing threads -- the slower side -- work.
+    int ring[Ctx::kStageDepth] = {};
+    int staged = 0;
     for (int k = 0; !rc && k < Ctx::kCopyChunks; ++k) {
       const int r0 = static_cast<int>(static_cast<int64_t>(n) * k / Ctx::kCopyChunks);
       const int r1 = static_cast<int>(static_cast<int64_t>(n) * (k + 1) / Ctx::kCopyChunks);
       if (r0 == r1) continue;
       const size_t off = static_cast<size_t>(r0) * n;
+      const bool pack = packed && k % 8 != 4;
       cudaError_t e;
-      if (packed) {
-        // the staging buffer this chunk uses was last copied two chunks ago
-        uint16_t *stage = c.h_stage[k & 1];
-        if (k >= 2 && cudaEventSynchronize(c.ev_chunk[k - 2]) != cudaSuccess) {
+      if (pack) {
+        // wait for the copy of the chunk that last used this staging buffer
+        const int slot = staged % Ctx::kStageDepth;
+        uint16_t *stage = c.h_stage[slot];
+        if (staged >= Ctx::kStageDepth && cudaEventSynchronize(c.ev_chunk[ring[slot]]) != cudaSuccess) {
           rc = c.fail_cuda("staging wait");
           break;
         }
+        ring[slot] = k;
+        ++staged;
         pack_rows(c, pref_w + off, stage, static_cast<size_t>(r1 - r0) * n, n);
         e = cudaMemcpyAsync(c.d_pw16.as<uint16_t>() + off, stage, sizeof(uint16_t) * static_cast<size_t>(r1 - r0) * n,
                             cudaMemcpyHostToDevice, c.copy_stream);
@@ -898,7 +907,7 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
         rc = c.fail_cuda("pref_w chunk copy");
         break;
       }
-      rc = packed ? enqueue_qinvert16(c, r0, r1) : enqueue_qinvert(c, r0, r1);
+      rc = pack ? enqueue_qinvert16(c, r0, r1) : enqueue_qinvert(c, r0, r1);
     }
     if (!rc && cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
     if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
@@ -909,7 +918,7 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
     if (!rc && c.h_ctrl->retry && !c.h_ctrl->status) {
       c.known_mode = -1;
       rc = copy_rest_of_m();
-      // the rank-mode retry inverts pref_w itself: the packed copy will not do
+      // the rank-mode retry inverts pref_w itself: the packed chunks will not do
       if (!rc && packed && cudaMemcpyAsync(dw, pref_w, row * n, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
         rc = c.fail_cuda("pref_w copy");
       if (!rc) rc = enqueue_retry_round<uint16_t>(c);
