@@ -56,6 +56,10 @@ def parse_args():
     ap.add_argument("--init-study", action="store_true",
                     help="the reference's init study (benchmark/figure_5.cu): its GPU init engine beside ours")
     ap.add_argument("--init-sizes", default="1000,5000,10000,15000,30000")
+    ap.add_argument("--bamboo-study", action="store_true",
+                    help="the reference's GPU engine SmpEngineBamboo beside ours on the same B200 and instances")
+    ap.add_argument("--bamboo-cases", default="0:2000:1,0:30000:2",
+                    help="kind:n:seed triples for --bamboo-study")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 8192-instance batched leg")
@@ -665,10 +669,114 @@ def run_init_study(args) -> None:
     ctx.close()
 
 
+def run_bamboo_study(args) -> None:
+    """The reference's own GPU engine, SmpEngineBamboo (the BambooSMP solve:
+    GPU rank and PR matrices, La3F9CoreKernel, a host monitor that finishes a
+    last lone chain on the CPU; src/smp/smp_engine_bamboo.cu), built from its
+    sources into oracle/_ref/libsmpref_bamboo{,_o3}.so, beside this library's
+    solve on the same B200 and the same instances.  The reference's figures
+    are its engine's own precheck/init/core stopwatch (AbsSmpEngine,
+    smp_engine_abs.h:10-36), with its untimed list upload and PR-matrix
+    download listed apart; ours are the device-input solve (CUDA events) and
+    the host-input solve through the C ABI (wall clock).  Matchings must be
+    identical.  One JSON line per case."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import pactae_b200 as pb
+
+    libs = {}
+    for tag, name in (("ptxas_O0_release", "libsmpref_bamboo.so"), ("ptxas_O3", "libsmpref_bamboo_o3.so")):
+        path = ROOT / "oracle" / "_ref" / name
+        if path.exists():
+            lib = ctypes.CDLL(str(path))
+            lib.ref_bamboo_solve.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                             ctypes.POINTER(ctypes.c_double)]
+            libs[tag] = lib
+    if not libs:
+        print(json.dumps({"bamboo_study": "unavailable", "why": "oracle/_ref/libsmpref_bamboo*.so not built"}))
+        return
+    def mem_available() -> int:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+        return 0
+
+    ctx = pb.Context(0)
+    for case in args.bamboo_cases.split(","):
+        kind, n, seed = (int(x) for x in case.split(":"))
+        # host bytes at peak: our pinned lists (8 n^2), the engine's SmpObj and
+        # its construction copies (16 n^2) and its host PR matrix (8 n^2)
+        need = 32 * n * n
+        if mem_available() < 2 * need:
+            print(json.dumps({"bamboo_study": f"kind {kind} n={n} seed {seed}", "unavailable":
+                              f"host memory: {mem_available() >> 30} GiB available, {2 * need >> 30} GiB wanted"}),
+                  flush=True)
+            continue
+        dpm, dpw = ctx.generate(kind, n, seed)
+        ours_match, _ = ctx.solve(dpm, dpw)  # warm-up
+        dev_ms = []
+        for _ in range(3):
+            _, st = ctx.solve(dpm, dpw)
+            dev_ms.append(st["total_ms"])
+        want = ours_match.cpu().numpy()
+        hpm_t = torch.empty((n, n), dtype=torch.int32, pin_memory=True)
+        hpw_t = torch.empty((n, n), dtype=torch.int32, pin_memory=True)
+        hpm_t.copy_(dpm)
+        hpw_t.copy_(dpw)
+        del dpm, dpw
+        torch.cuda.empty_cache()
+        hpm, hpw = hpm_t.numpy(), hpw_t.numpy()
+        hm = torch.empty(n, dtype=torch.int32, pin_memory=True).numpy()
+        ctx.solve(hpm, hpw, out=hm)
+        e2e_ms = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            ctx.solve(hpm, hpw, out=hm)
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        assert np.array_equal(hm, want), "host-input matching differs from the device-input one"
+        ref = {}
+        for tag, lib in libs.items():
+            runs = []
+            for _ in range(2):  # the first run warms the engine up
+                ms = (ctypes.c_double * 6)()
+                got = np.empty(n, np.int32)
+                rc = lib.ref_bamboo_solve(hpm.ctypes.data, hpw.ctypes.data, n, got.ctypes.data, ms)
+                runs.append((rc, list(ms), got))
+            rc, ms, got = runs[-1]
+            # engine-reported total: precheck + init + core with the lists
+            # already on the device (the engine's constructor uploads them,
+            # untimed); end to end: that upload plus FindStableMatching,
+            # which adds the untimed PR-matrix download and PostProc
+            ref[tag] = {"status": rc, "precheck_ms": round(ms[0], 3), "init_ms": round(ms[1], 3),
+                        "core_ms": round(ms[2], 3), "engine_total_ms": round(ms[0] + ms[1] + ms[2], 3),
+                        "untimed_upload_ms": round(ms[3], 1),
+                        "find_stable_matching_wall_ms": round(ms[4], 1),
+                        "end_to_end_ms": round(ms[3] + ms[4], 1),
+                        "matching_equal": bool(rc == 0 and np.array_equal(got, want)),
+                        "engine_total_ms_first_run": round(sum(runs[0][1][:3]), 3)}
+        best_dev = min(r["engine_total_ms"] for r in ref.values())
+        best_e2e = min(r["end_to_end_ms"] for r in ref.values())
+        print(json.dumps({"bamboo_study": f"kind {kind} n={n} seed {seed}", "n": n, "kind": kind, "seed": seed,
+                          "reference_smp_engine_bamboo": ref,
+                          "ours": {"device_input_ms": round(min(dev_ms), 3), "host_input_e2e_ms": round(min(e2e_ms), 2)},
+                          "speedup_vs_best_reference": {
+                              "device_input_vs_engine_total": round(best_dev / min(dev_ms), 1),
+                              "host_input_e2e_vs_end_to_end": round(best_e2e / min(e2e_ms), 1)}}), flush=True)
+        del hpm_t, hpw_t
+    ctx.close()
+
+
 def main():
     args = parse_args()
     if args.init_study:
         run_init_study(args)
+        return
+    if args.bamboo_study:
+        run_bamboo_study(args)
         return
     if args.impl == "reference":
         # Host-only arm: rank 0 times the reference's CPU engine; other ranks

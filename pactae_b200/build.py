@@ -83,7 +83,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
 
 def build_oracle(verbose: bool = False) -> None:
     """Compile the CPU oracle (test infrastructure) and, when the reference
-    sources are present, the reference's own CPU engines."""
+    sources are present, the reference's own CPU engines and the GPU engines
+    the studies time beside this library."""
     oracle = ROOT / "oracle"
     targets = ["all"]
     ref = Path(os.environ.get("SMP_REFERENCE_DIR", "/root/reference"))
@@ -91,6 +92,8 @@ def build_oracle(verbose: bool = False) -> None:
         targets.append("ref")
     if (ref / "include" / "smp" / "smp_init_3.h").exists():
         targets.append("ref-gpu")
+    if (ref / "src" / "smp" / "smp_engine_bamboo.cu").exists():
+        targets.append("ref-bamboo")
     cmd = ["make", "-s", "-C", str(oracle), *targets, f"REF={ref}"]
     if verbose:
         print(" ".join(cmd), flush=True)
