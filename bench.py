@@ -311,11 +311,15 @@ def run_b200(args, dist: Dist) -> dict | None:
         ms_per_step = total_ms / args.steps
         peak, peak_kind = measured_peak_hbm()
         P = st0["proposals"]
-        b_solve = 8 * n * n + 36 * P
+        swapped = st0["mode"] == 3
         # The roofline unit is one solve: B_alg = 8 n^2 (inversion: read
         # pref_w, write an int32 rank matrix) + 36 B per proposal (4 B of the
         # man's list + one 32 B sector of the rank matrix), over the device
-        # time of the whole solve.
+        # time of the whole solve.  When the men share one list the women
+        # propose instead: the men's n(n+1)/2 proposals are counted, not made,
+        # and the bytes the solve must move are both lists read once (the
+        # screen that proves the list is shared and pref_w valid).
+        b_solve = 8 * n * n if swapped else 8 * n * n + 36 * P
         solve_ach = b_solve / (ms_per_step * 1e-3) / 1e9
         query = st0["mode"] == 1
         K = 192
@@ -323,15 +327,21 @@ def run_b200(args, dist: Dist) -> dict | None:
         # the first K choices read twice, the bucket lists written and read,
         # the prefix written; rank mode: pref_w read, uint16 rank written,
         # prefix gathered)
-        init_bytes = (4 * n * n + 20 * n * K) if query else (4 * n * n + 2 * n * n + 36 * n * K)
+        if swapped:
+            init_bytes = 8 * n * n
+        elif query:
+            init_bytes = 4 * n * n + 20 * n * K
+        else:
+            init_bytes = 4 * n * n + 2 * n * n + 36 * n * K
         init_ms = statistics.mean(s["invert_ms"] for s in steps)
         init_ach = init_bytes / (init_ms * 1e-3) / 1e9
+        init_kernels = ("k_swap_pos, k_swap_screen" if swapped else
+                        "k_qcount, k_qscan, k_qscatter, k_qinvert" if query else "k_invert, k_prefix")
         phases = {
-            "init": {"ms": round(init_ms, 4), "kernels": "k_qcount, k_qscan, k_qscatter, k_qinvert" if query
-                     else "k_invert, k_prefix", "min_bytes": init_bytes, "achieved_gbs": round(init_ach, 1),
-                     "frac": round(init_ach / peak, 4), "bound": "hbm"},
-            "bulk": {"ms": round(st0["bulk_ms"], 4), "kernels": "k_bulk", "hops": st0["bulk_hops"],
-                     "bound": "latency (dependent L2 loads and atomics)"},
+            "init": {"ms": round(init_ms, 4), "kernels": init_kernels, "min_bytes": init_bytes,
+                     "achieved_gbs": round(init_ach, 1), "frac": round(init_ach / peak, 4), "bound": "hbm"},
+            "bulk": {"ms": round(st0["bulk_ms"], 4), "kernels": "k_swap_gs (the women propose)" if swapped
+                     else "k_bulk", "hops": st0["bulk_hops"], "bound": "latency (dependent L2 loads and atomics)"},
             "tail": {"ms": round(st0["tail_ms"], 4), "kernels": "k_tail_q" if query else "k_tail",
                      "hops": st0["tail_hops"], "bound": "latency (one SM, serial displacement chains)"},
         }
@@ -347,7 +357,8 @@ def run_b200(args, dist: Dist) -> dict | None:
             "traffic": traffic,
             "traffic_note": "DRAM bytes per solve from ncu (profiles/), scaled from n=12000" if traffic else None,
             "algorithmic_bytes_per_launch": b_solve,
-            "formula": "B_alg = 8 n^2 + 36 P over the solve's device time (CUDA events)",
+            "formula": ("B_alg = 8 n^2 (both lists read once; the women propose) over the solve's device time"
+                        if swapped else "B_alg = 8 n^2 + 36 P over the solve's device time (CUDA events)"),
             "launch_ms": round(ms_per_step, 4),
             "phases": phases,
         }

@@ -111,7 +111,7 @@ typedef struct smp_cfg {
   uint64_t hbm_budget;     /* bytes the batch / serving paths may hold resident;    */
                            /* 0 = 64 GiB                                            */
   int32_t tail_window;     /* the same for the tail kernel; 0 = auto                */
-  int32_t mode;            /* 0 = auto, 1 = rank-matrix mode only                   */
+  int32_t mode;            /* 0 = auto, 1 = the men's rank-matrix mode only         */
   uint64_t reserved[3];
 } smp_cfg;
 
@@ -126,7 +126,8 @@ typedef struct smp_stats {
   int32_t kernel_launches; /* kernels the call launched                            */
   int32_t bulk_hops;       /* accepted proposals in the all-SM kernel              */
   int32_t tail_hops;       /* accepted proposals in the tail kernel                */
-  int32_t mode;            /* 0 rank-matrix mode, 1 query mode, 2 query then rank  */
+  int32_t mode;            /* 0 rank-matrix mode, 1 query mode, 2 query then rank, */
+                           /* 3 the men share one list and the women proposed      */
   float stage_ms;          /* host->device copy of the inputs                       */
   float precheck_ms;       /* device time of each phase (CUDA events)              */
   float init_ms;

@@ -37,7 +37,7 @@ struct Control {
   int32_t distinct;       // precheck: number of distinct first choices
   int32_t distinct_w;     // k_wdistinct: distinct first choices of the women
   int32_t use_filter;     // k_wdistinct: k_bulk runs with its shared partner-rank filter
-  int32_t pad0;
+  int32_t swap_fail;      // k_swap_screen: a pref_m row differs from row 0
   unsigned long long proposals;        // sum over men of (final position + 1)
   unsigned long long blocking;         // checker: blocking pairs
   unsigned long long check_proposals;  // checker: proposals recounted from the matching
@@ -48,7 +48,7 @@ struct Control {
   // Chains k_tail handed to k_tail_coop (man, next position), at most one
   // per warp of the tail CTA; coop_count is 0 when none are waiting.
   int32_t coop_count;
-  int32_t pad1;
+  int32_t swap_next;      // k_swap_gs: next woman that has not proposed yet
   int2 coop_chain[32];
 };
 

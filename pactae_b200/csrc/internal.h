@@ -180,6 +180,7 @@ struct Ctx {
   int rank_bytes = 2;
   bool rank_valid = false;  // d_rank holds the inversion of pref_w
   bool tail_ran = false;
+  bool swapped = false;  // the men share one list and the women proposed
   int phase = 0;            // 0 staged, 1 prechecked, 2 inited, 3 cored, 4 posted
   // The mode the host has read back from the precheck (kModeQuery / kModeRank),
   // or -1: the enqueue functions then skip the kernels that mode would gate
@@ -188,6 +189,7 @@ struct Ctx {
 
   DeviceBuf d_pref_m, d_pref_w, d_rank, d_rankT, d_pr, d_prefix, d_bid, d_tailq, d_seen, d_ctrl, d_match;
   DeviceBuf d_pw16;  // pref_w packed to uint16 (host-input solves)
+  DeviceBuf d_swap_pos;  // women-proposing solves: position of each woman in the men's shared list
   // Host-input solves: a ring of pinned buffers the chunks of pref_w are
   // packed into while earlier ones are copied, and the threads that pack.
   static constexpr int kStageDepth = 3;
@@ -204,10 +206,10 @@ struct Ctx {
   static constexpr int kCopyChunks = 16;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_chunk[kCopyChunks] = {};
-  std::array<DeviceBuf *, 21> buffers() {
+  std::array<DeviceBuf *, 22> buffers() {
     return {&d_pref_m, &d_pref_w, &d_pw16, &d_rank,    &d_rankT,    &d_pr,     &d_prefix, &d_bid,    &d_tailq,
             &d_seen,   &d_ctrl,   &d_match,   &d_husband,  &d_prank,  &d_qcnt,   &d_qlist,
-            &gen_keys_a, &gen_keys_b, &gen_seg, &gen_temp, &gen_aux};
+            &gen_keys_a, &gen_keys_b, &gen_seg, &gen_temp, &gen_aux, &d_swap_pos};
   }
   int launches = 0;  // kernels launched since the last stage / call
   smp_stats stats = {};

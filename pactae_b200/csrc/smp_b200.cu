@@ -11,6 +11,7 @@
 #include "common.cuh"
 #include "internal.h"
 #include "solve_kernels.cuh"
+#include "swap_kernels.cuh"
 
 using namespace smpb200;
 
@@ -526,6 +527,7 @@ int stage_reset(Ctx &c, int32_t n) {
   c.stats.blocking_pairs = -1;
   c.launches = 0;
   c.known_mode = -1;
+  c.swapped = false;
   plan(c);
   return SMP_OK;
 }
@@ -567,8 +569,8 @@ void fill_stats(Ctx &c, bool timed_phases) {
   c.stats.bulk_hops = static_cast<int32_t>(c.h_ctrl->bulk_hops);
   c.stats.tail_hops = static_cast<int32_t>(c.h_ctrl->tail_hops);
   c.stats.perfect = c.h_ctrl->perfect;
-  c.stats.mode = c.h_ctrl->retry ? 2 : c.h_ctrl->mode;
-  c.stats.tail_men = c.tail_ran ? c.h_ctrl->tail_men : 0;
+  c.stats.mode = c.swapped ? 3 : c.h_ctrl->retry ? 2 : c.h_ctrl->mode;
+  c.stats.tail_men = c.tail_ran && !c.swapped ? c.h_ctrl->tail_men : 0;
   c.stats.rank_bytes = c.rank_bytes;
   c.stats.kernel_launches = c.launches;
   if (timed_phases) {
@@ -583,7 +585,7 @@ void fill_stats(Ctx &c, bool timed_phases) {
   if (c.phase >= 3 && !c.h_ctrl->perfect) {
     c.stats.invert_ms = elapsed(c, kEvPrecheckEnd, kEvInvertEnd);
     c.stats.bulk_ms = elapsed(c, kEvInitEnd, kEvBulkEnd);
-    c.stats.tail_ms = c.tail_ran ? elapsed(c, kEvBulkEnd, kEvCoreEnd) : 0.f;
+    c.stats.tail_ms = c.tail_ran && !c.swapped ? elapsed(c, kEvBulkEnd, kEvCoreEnd) : 0.f;
   }
 }
 
@@ -689,6 +691,8 @@ int solve_enqueue(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t 
 // keep their gates, so the device still decides what runs.  The checker
 // (SMP_F_CHECK) must see the final matching: those solves take the fully
 // gated pipeline.
+int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped);
+
 int solve_staged(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
                  uint32_t flags, smp_stats *st) {
   // the checker, a disabled tail or a configured tail window (whose tail
@@ -731,19 +735,80 @@ int solve_staged(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n
   const bool done = speculate && !h.status && (h.perfect || (h.mode == kModeQuery && !h.retry));
   if (!done && !h.status) {
     // pass 2: the rank mode, or the rank-mode retry of a query-mode round 0
+    bool swapped = false;
     if (speculate && h.mode == kModeQuery && h.retry) {
       c.known_mode = -1;
       rc = c.rank_bytes == 2 ? enqueue_retry_round<uint16_t>(c) : enqueue_retry_round<int32_t>(c);
     } else {
-      c.known_mode = h.perfect ? -1 : h.mode;
-      rc = enqueue_init(c);
-      if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-      if (!rc) rc = enqueue_core(c);
+      // one first choice for every man: perhaps one list for every man
+      if (!h.perfect && h.mode == kModeRank && h.distinct == 1 && n >= 2 && c.mode_cfg == 0)
+        rc = solve_swapped(c, flags, match_out, swapped);
+      if (!rc && !swapped) {
+        c.known_mode = h.perfect ? -1 : h.mode;
+        rc = enqueue_init(c);
+        if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+        if (!rc) rc = enqueue_core(c);
+      }
     }
-    if (!rc) rc = finish_pass();
+    if (!rc && !swapped) rc = finish_pass();
     if (rc) return rc;
   }
   return solve_finish(c, flags, st);
+}
+
+// A rank-mode solve whose men all make the same first choice may have men
+// who share one list.  The screen checks that on all SMs (and that pref_w's
+// rows are permutations); if so, the women propose and `swapped` is set,
+// else the caller runs the men's rank-mode pass.  Stops after the screen,
+// with `swapped` set, when it found invalid input.
+int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped) {
+  swapped = false;
+  const int n = c.n;
+  const size_t words = (static_cast<size_t>(n) + 31) / 32;
+  if (words * 4 > c.smem_optin) return SMP_OK;
+  int rc = c.d_swap_pos.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (!rc) rc = c.d_bid.ensure(sizeof(unsigned long long) * static_cast<size_t>(n));
+  if (!rc) rc = c.d_match.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (rc) return rc;
+  Control *ctrl = c.d_ctrl.as<Control>();
+  int32_t *pos = c.d_swap_pos.as<int32_t>();
+  unsigned long long *bid = c.d_bid.as<unsigned long long>();
+  const int grid = std::max(1, std::min(c.sm_count * 4, (n + 255) / 256));
+  if (cudaMemsetAsync(pos, 0xFF, sizeof(int32_t) * static_cast<size_t>(n), c.stream) != cudaSuccess)
+    return c.fail_cuda("swap reset");
+  k_swap_pos<<<grid, 256, 0, c.stream>>>(c.pref_m, pos, n, ctrl);
+  if (allow_dynamic_smem(c, k_swap_screen) != cudaSuccess) return c.fail_cuda("k_swap_screen smem attribute");
+  k_swap_screen<<<std::min(2 * n, c.sm_count * 8), 256, words * 4, c.stream>>>(c.pref_m, c.pref_w, n, ctrl);
+  c.launches += 2;
+  rc = c.check_launch("k_swap_screen");
+  if (!rc && cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = read_control(c);
+  if (!rc) rc = c.sync("swap screen");
+  if (rc) return rc;
+  if (c.h_ctrl->status) {
+    swapped = true;
+    return SMP_OK;
+  }
+  if (c.h_ctrl->swap_fail) return SMP_OK;
+  swapped = true;
+  c.swapped = true;
+  if (cudaMemsetAsync(bid, 0xFF, sizeof(unsigned long long) * static_cast<size_t>(n), c.stream) != cudaSuccess)
+    return c.fail_cuda("swap bid reset");
+  if (cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  k_swap_gs<<<c.sm_count * 4, 256, 0, c.stream>>>(c.pref_m, c.pref_w, pos, bid, n, ctrl);
+  c.launches++;
+  rc = c.check_launch("k_swap_gs");
+  if (!rc && cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc && cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (rc) return rc;
+  k_swap_match<<<grid, 256, 0, c.stream>>>(c.pref_m, bid, c.d_match.as<int32_t>(), n, ctrl);
+  c.launches++;
+  rc = c.check_launch("k_swap_match");
+  if (!rc) rc = copy_match_out(c, match_out, (flags & SMP_F_DEVICE_PTRS) != 0);
+  if (!rc && cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = read_control(c);
+  if (!rc) rc = c.sync("solve");
+  return rc;
 }
 
 // Statistics and status of a solve whose stream has completed.
@@ -859,6 +924,7 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
   };
   const bool query = c.h_ctrl->mode == kModeQuery && !c.h_ctrl->perfect;
   if (!c.h_ctrl->perfect) c.known_mode = c.h_ctrl->mode;  // enqueue only this mode's kernels
+  bool swapped = false;
   if (!query) {
     if (!c.h_ctrl->perfect) {
       rc = copy_rest_of_m();
@@ -866,9 +932,12 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
         rc = c.fail_cuda("pref_w copy");
     }
     if (!rc && cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-    if (!rc) rc = enqueue_init(c);
-    if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-    if (!rc) rc = enqueue_core(c);
+    // one first choice for every man: perhaps one list for every man
+    if (!rc && !c.h_ctrl->perfect && c.h_ctrl->mode == kModeRank && c.h_ctrl->distinct == 1 && c.mode_cfg == 0)
+      rc = solve_swapped(c, flags, match_out, swapped);
+    if (!rc && !swapped) rc = enqueue_init(c);
+    if (!rc && !swapped && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    if (!rc && !swapped) rc = enqueue_core(c);
   } else {
     if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
     rc = init_buffers(c);
@@ -924,11 +993,13 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
       if (!rc) rc = enqueue_retry_round<uint16_t>(c);
     }
   }
-  if (!rc && cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-  if (!rc) rc = enqueue_post(c);
-  if (!rc && cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-  if (!rc) rc = copy_match_out(c, match_out, false);
-  if (!rc) rc = read_control(c);
+  if (!swapped) {  // the women-proposing pass has finished its solve
+    if (!rc && cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    if (!rc) rc = enqueue_post(c);
+    if (!rc && cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    if (!rc) rc = copy_match_out(c, match_out, false);
+    if (!rc) rc = read_control(c);
+  }
   // Both streams drain before returning, even after an error: the copies
   // read the caller's buffers.
   const int rs = c.sync("solve");

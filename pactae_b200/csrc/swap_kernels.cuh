@@ -1,0 +1,178 @@
+// Single solves whose men all share one list: the women propose.
+//
+// When every man ranks the women in the same order L, the stable matching is
+// unique (each woman, taken in L's order, gets her best man not taken by a
+// woman before her), so the women-proposing run returns the matching the
+// men-proposing Gale-Shapley of the reference returns
+// (src/smp/smp_engine_gs_1.cu:47-98).  The men's run would make n(n+1)/2
+// proposals -- the man who ends with L[k] proposed to L[0..k] -- and needs the
+// full rank matrix; the women's run makes about n ln n proposals and ranks
+// every proposer by one inverted row, pos[w] = position of w in L.
+//
+//   k_swap_pos     pos = inverse of pref_m row 0; row 0 must be a permutation
+//   k_swap_screen  every pref_m row equals row 0 (else swap_fail), and every
+//                  pref_w row is a permutation (else the invalid-input status)
+//   k_swap_gs      the women's proposals, one warp per chain
+//   k_swap_match   match[m] from the men's final bids; the men's proposal count
+#pragma once
+
+#include "common.cuh"
+#include "solve_kernels.cuh"
+
+namespace smpb200 {
+
+// pos[L[r]] = r, with pos preset to -1; an entry out of range or seen twice
+// makes row 0 no permutation.
+__global__ void k_swap_pos(const int32_t *__restrict__ pref_m, int32_t *__restrict__ pos, int n, Control *ctrl) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int w = __ldg(pref_m + r);
+    if (static_cast<unsigned>(w) >= static_cast<unsigned>(n) || atomicCAS(pos + w, -1, r) != -1)
+      report(ctrl, kStatusInvalidInput, w);
+  }
+}
+
+// Rows t = 1 .. n-1 compare pref_m row t with row 0; rows t = n .. 2n-1
+// check that pref_w row t-n is a permutation with a shared bitmap.  Row
+// bodies move in 16-byte loads (row_span: rows start off 16-byte boundaries
+// when n is not a multiple of 4).  Once a pref_m row differs, the solve takes
+// the men's rank-mode pass, which checks pref_w itself: the CTAs stop.
+__global__ void __launch_bounds__(256) k_swap_screen(const int32_t *__restrict__ pref_m,
+                                                     const int32_t *__restrict__ pref_w, int n, Control *ctrl) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t *seen = reinterpret_cast<uint32_t *>(smem_raw);
+  __shared__ int s_stop;
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;
+  const int words = (n + 31) >> 5;
+  bool bad = false;
+  int bad_value = 0;
+  for (int t = 1 + static_cast<int>(blockIdx.x); t < 2 * n; t += gridDim.x) {
+    if (tid == 0) s_stop = ld_volatile_s32(&ctrl->swap_fail) || ld_volatile_s32(&ctrl->status);
+    __syncthreads();
+    if (s_stop) break;
+    if (t < n) {
+      // pref_m row t against row 0, element by element
+      const RowSpan s = row_span(pref_m, t, n);
+      bool differs = false;
+      for (int i = tid; i < s.nq; i += nthr) {
+        const int4 v = __ldcs(s.rq + i);
+        const int c = s.head + 4 * i;
+        differs |= v.x != __ldg(pref_m + c) || v.y != __ldg(pref_m + c + 1) || v.z != __ldg(pref_m + c + 2) ||
+                   v.w != __ldg(pref_m + c + 3);
+      }
+      if (tid < s.head) differs |= __ldcs(s.row + tid) != __ldg(pref_m + tid);
+      const int c0 = s.head + 4 * s.nq;
+      if (tid < s.tail) differs |= __ldcs(s.row + c0 + tid) != __ldg(pref_m + c0 + tid);
+      if (__syncthreads_or(differs) && tid == 0) atomicExch(&ctrl->swap_fail, 1);
+    } else {
+      // pref_w row t - n: every value in range and seen once
+      for (int i = tid; i < words; i += nthr) seen[i] = 0u;
+      __syncthreads();
+      const RowSpan s = row_span(pref_w, t - n, n);
+      const auto mark = [&](int v) {
+        if (static_cast<unsigned>(v) >= static_cast<unsigned>(n)) {
+          bad = true;
+          bad_value = v;
+          return;
+        }
+        const uint32_t bit = 1u << (v & 31);
+        if (atomicOr(seen + (v >> 5), bit) & bit) {
+          bad = true;
+          bad_value = v;
+        }
+      };
+      for (int i = tid; i < s.nq; i += nthr) {
+        const int4 v = __ldcs(s.rq + i);
+        mark(v.x);
+        mark(v.y);
+        mark(v.z);
+        mark(v.w);
+      }
+      if (tid < s.head) mark(__ldcs(s.row + tid));
+      if (tid < s.tail) mark(__ldcs(s.row + s.head + 4 * s.nq + tid));
+      __syncthreads();  // the bitmap is cleared for the next row only after this one
+    }
+  }
+  if (bad) report(ctrl, kStatusInvalidInput, bad_value);
+}
+
+// The women's proposals.  A man's bid word is pos[w] << 32 | r for the woman
+// w he holds and her position r in her list (~0 while he is free), so
+// atomicMin keeps the woman the men prefer and hands back the one it
+// displaced together with where she resumes.  Each warp carries one woman:
+// her next 32 men are read at once, the first man whose current word is
+// worse than hers takes her proposal, and a displaced woman continues in the
+// same warp.  A woman runs out of men only on input that is not a
+// permutation, which the screen has excluded; the bound keeps every read in
+// her row regardless.
+__global__ void __launch_bounds__(256) k_swap_gs(const int32_t *__restrict__ pref_m,
+                                                 const int32_t *__restrict__ pref_w,
+                                                 const int32_t *__restrict__ pos,
+                                                 unsigned long long *__restrict__ bid, int n, Control *ctrl) {
+  const int lane = threadIdx.x & 31;
+  int w = -1, r0 = 0;
+  uint32_t key = 0;
+  for (;;) {
+    if (w < 0) {
+      int i = 0;
+      if (lane == 0) i = atomicAdd(&ctrl->swap_next, 1);
+      i = __shfl_sync(kFullMask, i, 0);
+      if (i >= n) break;
+      w = i;
+      r0 = 0;
+      key = static_cast<uint32_t>(__ldg(pos + w));
+    }
+    if (r0 >= n) {
+      if (lane == 0) report(ctrl, kStatusInvalidInput, w);
+      w = -1;
+      continue;
+    }
+    const int r = r0 + lane;
+    const int m = r < n ? __ldg(pref_w + static_cast<size_t>(w) * n + r) : 0;
+    const bool open = r < n && static_cast<unsigned>(m) < static_cast<unsigned>(n) &&
+                      static_cast<uint32_t>(ld_relaxed_u64(bid + m) >> 32) > key;
+    const unsigned hit = __ballot_sync(kFullMask, open);
+    if (!hit) {
+      r0 += 32;
+      continue;
+    }
+    const int f = __ffs(hit) - 1;
+    unsigned long long old = 0;
+    if (lane == f)
+      old = atomicMin(bid + m, (static_cast<unsigned long long>(key) << 32) | static_cast<uint32_t>(r));
+    old = __shfl_sync(kFullMask, old, f);
+    if (static_cast<uint32_t>(old >> 32) < key) {  // a woman the men prefer got there first
+      r0 += f + 1;
+      continue;
+    }
+    if (old == ~0ull) {  // he was free: the chain ends
+      w = -1;
+      continue;
+    }
+    key = static_cast<uint32_t>(old >> 32);
+    w = __ldg(pref_m + key);
+    r0 = static_cast<int>(old & 0xFFFFFFFFull) + 1;
+  }
+}
+
+// match[m] = the woman m holds; the men's proposal count of the same
+// matching is n(n+1)/2 (final positions 0 .. n-1 in the shared list).
+__global__ void k_swap_match(const int32_t *__restrict__ pref_m, const unsigned long long *__restrict__ bid,
+                             int32_t *__restrict__ match, int n, Control *ctrl) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+    const unsigned long long b = bid[m];
+    if (b == ~0ull) {
+      report(ctrl, kStatusInvalidInput, m);
+      match[m] = -1;
+    } else {
+      match[m] = __ldg(pref_m + static_cast<uint32_t>(b >> 32));
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctrl->proposals = static_cast<unsigned long long>(n) * (static_cast<unsigned long long>(n) + 1) / 2;
+    ctrl->bulk_proposals = ctrl->proposals;
+    ctrl->tail_proposals = 0;
+  }
+}
+
+}  // namespace smpb200

@@ -31,7 +31,7 @@ def sha(a) -> str:
 
 
 def to_host(t) -> np.ndarray:
-    return t.cpu().numpy()
+    return t if isinstance(t, np.ndarray) else t.cpu().numpy()
 
 
 # -- generator --------------------------------------------------------------
@@ -110,7 +110,7 @@ def test_pipeline_variants_agree(prefix_k, tail):
 @pytest.mark.parametrize("kind,param,prefix_k,mode", [
     (pb.SMP_GEN_UNIFORM, 0, 0, 1),        # query mode: pref_w arrives in row chunks
     (pb.SMP_GEN_UNIFORM, 0, 8, 2),        # men go beyond an 8-choice prefix: the rest of pref_m follows
-    (pb.SMP_GEN_CONGESTED, 0, 0, 0),      # rank mode: everything is copied first
+    (pb.SMP_GEN_CONGESTED, 0, 0, 3),      # everything is copied first; the men share one list: women propose
     (pb.SMP_GEN_CORRELATED, 500, 0, None),
     (pb.SMP_GEN_PERFECT, 0, 0, None),     # perfect: only the first choices are read
 ])
@@ -264,14 +264,27 @@ def test_deep_chain_families_match_oracle(ctx, kind, n, param):
     assert st["blocking_pairs"] == 0
 
 
+def twist(pm):
+    """One man swaps his last two choices: the men no longer share one list."""
+    pm = pm.copy()
+    n = pm.shape[0]
+    pm[n // 2, [n - 2, n - 1]] = pm[n // 2, [n - 1, n - 2]]
+    return pm
+
+
+@pytest.mark.parametrize("shared", [True, False])
 @pytest.mark.parametrize("where", ["man_deep", "man_first_choices", "woman_row"])
-def test_rank_mode_rejects_bad_entries(ctx, where):
-    # Congested lists take the rank mode: inversion, transpose, ranks by
-    # position.  A bad entry anywhere must end the solve with the status, and
-    # the context must solve the intact instance afterwards.
+def test_rank_mode_rejects_bad_entries(ctx, where, shared):
+    # Congested lists: men alike in every first choice.  With one shared list
+    # the women propose after a screen of both lists; with one man's list
+    # twisted the screen hands over to the men's rank mode (inversion,
+    # transpose, ranks by position).  A bad entry anywhere must end the solve
+    # with the status -- a bad man's row also differs from row 0, so those
+    # cases reach the rank mode -- and the context must solve the intact
+    # instance afterwards.
     n = 1001
     pm, pw = oracle.generate(pb.SMP_GEN_CONGESTED, n, 5)
-    pm = pm.copy()
+    pm = pm.copy() if shared else twist(pm)
     pw = pw.copy()
     if where == "man_deep":
         pm[7, 900] = n + 3
@@ -283,10 +296,43 @@ def test_rank_mode_rejects_bad_entries(ctx, where):
         ctx.solve(pm, pw)
     assert e.value.status == pb.SMP_ERR_INVALID_INPUT
     pm2, pw2 = oracle.generate(pb.SMP_GEN_CONGESTED, n, 5)
+    if not shared:
+        pm2 = twist(pm2)
     match, st = ctx.solve(pm2, pw2)
     want, props = oracle.gs_seq(pm2, pw2)
     assert np.array_equal(match, want) and st["proposals"] == props
-    assert st["mode"] == 0
+    assert st["mode"] == (3 if shared else 0)
+
+
+@pytest.mark.parametrize("kind,n,device", [
+    (pb.SMP_GEN_CONGESTED, 2, False),
+    (pb.SMP_GEN_CONGESTED, 3, False),
+    (pb.SMP_GEN_CONGESTED, 17, False),
+    (pb.SMP_GEN_CONGESTED, 1001, False),
+    (pb.SMP_GEN_REF_CONGESTED, 999, False),   # both sides share one list
+    (pb.SMP_GEN_CONGESTED, 4095, True),
+    (pb.SMP_GEN_CONGESTED, 6001, True),        # rows start off 16-byte boundaries
+    (pb.SMP_GEN_REF_CONGESTED, 5000, True),
+])
+def test_men_sharing_one_list_women_propose(ctx, kind, n, device):
+    # All men share one list: the stable matching is unique and the women
+    # propose; the matching and the men's proposal count n(n+1)/2 must equal
+    # the oracle's men-proposing run.
+    if device:
+        pm, pw = ctx.generate(kind, n, seed=13)
+    else:
+        pm, pw = oracle.generate(kind, n, 13)
+    match, st = ctx.solve(pm, pw)
+    want, props = oracle.gs_seq(to_host(pm), to_host(pw))
+    assert np.array_equal(to_host(match), want)
+    assert st["proposals"] == props == n * (n + 1) // 2
+    # up to n = 4 one distinct first choice in four already picks the query mode
+    assert st["mode"] == (3 if n > 4 else 1)
+    # a twisted list goes to the men's rank mode with the same answer as the oracle
+    pm2 = twist(to_host(pm))
+    match2, st2 = ctx.solve(pm2, to_host(pw))
+    want2, props2 = oracle.gs_seq(pm2, to_host(pw))
+    assert np.array_equal(match2, want2) and st2["proposals"] == props2 and st2["mode"] != 3
 
 
 def test_bad_arguments(ctx):
