@@ -764,8 +764,8 @@ int solve_staged(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n
 int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped) {
   swapped = false;
   const int n = c.n;
-  const size_t words = (static_cast<size_t>(n) + 31) / 32;
-  if (words * 4 > c.smem_optin) return SMP_OK;
+  const size_t screen_smem = swap_screen_smem(n);
+  if (screen_smem > c.smem_optin) return SMP_OK;
   int rc = c.d_swap_pos.ensure(sizeof(int32_t) * static_cast<size_t>(n));
   if (!rc) rc = c.d_bid.ensure(sizeof(unsigned long long) * static_cast<size_t>(n));
   if (!rc) rc = c.d_match.ensure(sizeof(int32_t) * static_cast<size_t>(n));
@@ -778,7 +778,13 @@ int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped) {
     return c.fail_cuda("swap reset");
   k_swap_pos<<<grid, 256, 0, c.stream>>>(c.pref_m, pos, n, ctrl);
   if (allow_dynamic_smem(c, k_swap_screen) != cudaSuccess) return c.fail_cuda("k_swap_screen smem attribute");
-  k_swap_screen<<<std::min(2 * n, c.sm_count * 8), 256, words * 4, c.stream>>>(c.pref_m, c.pref_w, n, ctrl);
+  int per_sm = 0;  // one wave: every CTA resident
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_swap_screen, 256, screen_smem) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  k_swap_screen<<<std::min(2 * n, c.sm_count * std::max(per_sm, 1)), 256, screen_smem, c.stream>>>(
+      c.pref_m, c.pref_w, n, ctrl);
   c.launches += 2;
   rc = c.check_launch("k_swap_screen");
   if (!rc && cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");

@@ -273,7 +273,8 @@ def twist(pm):
 
 
 @pytest.mark.parametrize("shared", [True, False])
-@pytest.mark.parametrize("where", ["man_deep", "man_first_choices", "woman_row"])
+@pytest.mark.parametrize("where", ["man_deep", "man_first_choices", "woman_row", "woman_out_of_range",
+                                   "woman_last_row"])
 def test_rank_mode_rejects_bad_entries(ctx, where, shared):
     # Congested lists: men alike in every first choice.  With one shared list
     # the women propose after a screen of both lists; with one man's list
@@ -290,8 +291,12 @@ def test_rank_mode_rejects_bad_entries(ctx, where, shared):
         pm[7, 900] = n + 3
     elif where == "man_first_choices":
         pm[11, 3] = -2
-    else:
+    elif where == "woman_row":
         pw[20, 10] = pw[20, 11]
+    elif where == "woman_out_of_range":
+        pw[30, 5] = n + 7
+    else:  # the last row, its last entries: the partial 16-byte word of the check
+        pw[n - 1, n - 1] = pw[n - 1, n - 2]
     with pytest.raises(pb.SmpError) as e:
         ctx.solve(pm, pw)
     assert e.value.status == pb.SMP_ERR_INVALID_INPUT
