@@ -49,6 +49,8 @@ struct Control {
   // per warp of the tail CTA; coop_count is 0 when none are waiting.
   int32_t coop_count;
   int32_t swap_next;      // k_swap_gs: next woman that has not proposed yet
+  int32_t w_differ;       // k_swap_screen: a pref_w row differs from row 0
+  int32_t pad1;
   int2 coop_chain[32];
 };
 

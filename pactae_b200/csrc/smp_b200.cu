@@ -798,18 +798,27 @@ int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped) {
   if (c.h_ctrl->swap_fail) return SMP_OK;
   swapped = true;
   c.swapped = true;
-  if (cudaMemsetAsync(bid, 0xFF, sizeof(unsigned long long) * static_cast<size_t>(n), c.stream) != cudaSuccess)
-    return c.fail_cuda("swap bid reset");
-  if (cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
-  k_swap_gs<<<c.sm_count * 4, 256, 0, c.stream>>>(c.pref_m, c.pref_w, pos, bid, n, ctrl);
-  c.launches++;
-  rc = c.check_launch("k_swap_gs");
-  if (!rc && cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-  if (!rc && cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-  if (rc) return rc;
-  k_swap_match<<<grid, 256, 0, c.stream>>>(c.pref_m, bid, c.d_match.as<int32_t>(), n, ctrl);
-  c.launches++;
-  rc = c.check_launch("k_swap_match");
+  if (!c.h_ctrl->w_differ) {  // the women share one list too: pair rank for rank
+    if (cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+    if (cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+    if (cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+    k_swap_direct<<<grid, 256, 0, c.stream>>>(c.pref_m, c.pref_w, c.d_match.as<int32_t>(), n, ctrl);
+    c.launches++;
+    rc = c.check_launch("k_swap_direct");
+  } else {
+    if (cudaMemsetAsync(bid, 0xFF, sizeof(unsigned long long) * static_cast<size_t>(n), c.stream) != cudaSuccess)
+      return c.fail_cuda("swap bid reset");
+    if (cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+    k_swap_gs<<<c.sm_count * 4, 256, 0, c.stream>>>(c.pref_m, c.pref_w, pos, bid, n, ctrl);
+    c.launches++;
+    rc = c.check_launch("k_swap_gs");
+    if (!rc && cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    if (!rc && cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+    if (rc) return rc;
+    k_swap_match<<<grid, 256, 0, c.stream>>>(c.pref_m, bid, c.d_match.as<int32_t>(), n, ctrl);
+    c.launches++;
+    rc = c.check_launch("k_swap_match");
+  }
   if (!rc) rc = copy_match_out(c, match_out, (flags & SMP_F_DEVICE_PTRS) != 0);
   if (!rc && cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
   if (!rc) rc = read_control(c);

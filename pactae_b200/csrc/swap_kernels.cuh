@@ -14,6 +14,9 @@
 //                  pref_w row is a permutation (else the invalid-input status)
 //   k_swap_gs      the women's proposals, one warp per chain
 //   k_swap_match   match[m] from the men's final bids; the men's proposal count
+//   k_swap_direct  women who share one list M as well: match[M[k]] = L[k]
+//                  (the k-th man of the women's list with the k-th woman of
+//                  the men's), no proposals
 #pragma once
 
 #include "common.cuh"
@@ -45,13 +48,17 @@ __global__ void __launch_bounds__(256) k_swap_screen(const int32_t *__restrict__
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint32_t *seen = reinterpret_cast<uint32_t *>(smem_raw);
   __shared__ int s_stop;
+  __shared__ int s_wsame;  // no pref_w row has differed from row 0 yet
   const int tid = threadIdx.x;
   const int nthr = blockDim.x;
   const int words = (n + 31) >> 5;
   bool bad = false;
   int bad_value = 0;
   for (int t = 1 + static_cast<int>(blockIdx.x); t < 2 * n; t += gridDim.x) {
-    if (tid == 0) s_stop = ld_volatile_s32(&ctrl->swap_fail) || ld_volatile_s32(&ctrl->status);
+    if (tid == 0) {
+      s_stop = ld_volatile_s32(&ctrl->swap_fail) || ld_volatile_s32(&ctrl->status);
+      s_wsame = !ld_volatile_s32(&ctrl->w_differ);
+    }
     __syncthreads();
     if (s_stop) break;
     if (t < n) {
@@ -80,10 +87,25 @@ __global__ void __launch_bounds__(256) k_swap_screen(const int32_t *__restrict__
       if (tid < s.tail) differs |= __ldcs(s.row + c0 + tid) != __ldg(pref_m + c0 + tid);
       if (__syncthreads_or(differs) && tid == 0) atomicExch(&ctrl->swap_fail, 1);
     } else {
-      // pref_w row t - n: every value in range and seen once
+      // pref_w row t - n: every value in range and seen once; while no
+      // row has differed, also compared with row 0 (the women may share one
+      // list as well)
       for (int i = tid; i < words; i += nthr) seen[i] = 0u;
       __syncthreads();
       const RowSpan s = row_span(pref_w, t - n, n);
+      if (s_wsame && t > n) {
+        bool differs = false;
+        for (int i = tid; i < s.nq; i += nthr) {
+          const int4 v = __ldcs(s.rq + i);
+          const int c = s.head + 4 * i;
+          differs |= v.x != __ldg(pref_w + c) || v.y != __ldg(pref_w + c + 1) || v.z != __ldg(pref_w + c + 2) ||
+                     v.w != __ldg(pref_w + c + 3);
+        }
+        if (tid < s.head) differs |= __ldcs(s.row + tid) != __ldg(pref_w + tid);
+        const int c0 = s.head + 4 * s.nq;
+        if (tid < s.tail) differs |= __ldcs(s.row + c0 + tid) != __ldg(pref_w + c0 + tid);
+        if (differs) atomicExch(&ctrl->w_differ, 1);
+      }
       const auto mark = [&](int v) {
         if (static_cast<unsigned>(v) >= static_cast<unsigned>(n)) {
           bad = true;
@@ -183,6 +205,20 @@ __global__ void k_swap_match(const int32_t *__restrict__ pref_m, const unsigned 
       match[m] = __ldg(pref_m + static_cast<uint32_t>(b >> 32));
     }
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctrl->proposals = static_cast<unsigned long long>(n) * (static_cast<unsigned long long>(n) + 1) / 2;
+    ctrl->bulk_proposals = ctrl->proposals;
+    ctrl->tail_proposals = 0;
+  }
+}
+
+// Both sides share one list each (L for the men, M for the women): the k-th
+// man of M and the k-th woman of L pair up.  The men's proposal count is
+// again n(n+1)/2.
+__global__ void k_swap_direct(const int32_t *__restrict__ pref_m, const int32_t *__restrict__ pref_w,
+                              int32_t *__restrict__ match, int n, Control *ctrl) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    match[__ldg(pref_w + k)] = __ldg(pref_m + k);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     ctrl->proposals = static_cast<unsigned long long>(n) * (static_cast<unsigned long long>(n) + 1) / 2;
     ctrl->bulk_proposals = ctrl->proposals;

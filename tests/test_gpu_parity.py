@@ -333,6 +333,13 @@ def test_men_sharing_one_list_women_propose(ctx, kind, n, device):
     assert st["proposals"] == props == n * (n + 1) // 2
     # up to n = 4 one distinct first choice in four already picks the query mode
     assert st["mode"] == (3 if n > 4 else 1)
+    if kind == pb.SMP_GEN_REF_CONGESTED:
+        # the women share one list too (paired rank for rank); with one
+        # woman's list twisted they propose instead
+        pw3 = twist(to_host(pw))
+        match3, st3 = ctx.solve(to_host(pm), pw3)
+        want3, props3 = oracle.gs_seq(to_host(pm), pw3)
+        assert np.array_equal(match3, want3) and st3["proposals"] == props3 and st3["mode"] == 3
     # a twisted list goes to the men's rank mode with the same answer as the oracle
     pm2 = twist(to_host(pm))
     match2, st2 = ctx.solve(pm2, to_host(pw))
