@@ -112,6 +112,32 @@ def test_congested_men_proposal_count():
     assert props == n * (n + 1) // 2
 
 
+@pytest.mark.parametrize("n,seed,women", [(40, 1, "uniform"), (301, 2, "uniform"), (257, 3, "correlated")])
+def test_shared_men_list_has_one_stable_matching(n, seed, women):
+    # The women-proposing solve of instances whose men share one list L
+    # rests on this: the men-proposing and the women-proposing runs agree,
+    # and both equal the serial dictatorship in which each woman, taken in
+    # L's order, takes her best man still untaken.
+    pm, _ = oracle.generate(oracle.GEN_CONGESTED, n, seed)
+    if women == "uniform":
+        _, pw = oracle.generate(oracle.GEN_UNIFORM, n, seed + 10)
+    else:
+        _, pw = oracle.generate(oracle.GEN_CORRELATED, n, seed + 10, 0, 500)
+    assert (pm == pm[0]).all()
+    men, _ = oracle.gs_seq(pm, pw)
+    wives, _ = oracle.gs_seq(pw, pm)  # the women propose: wives[w] = her man
+    from_women = np.empty(n, dtype=np.int32)
+    from_women[wives] = np.arange(n, dtype=np.int32)
+    assert np.array_equal(men, from_women)
+    taken = np.zeros(n, dtype=bool)
+    dictator = np.empty(n, dtype=np.int32)
+    for w in pm[0]:
+        m = next(int(x) for x in pw[w] if not taken[x])
+        taken[m] = True
+        dictator[m] = w
+    assert np.array_equal(men, dictator)
+
+
 def test_correlated_is_skewed_toward_high_scores():
     n = 400
     pm, _ = oracle.generate(oracle.GEN_CORRELATED, n, 4, 0, 500)
