@@ -14,6 +14,7 @@ Two libraries:
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 from pathlib import Path
 
@@ -33,6 +34,17 @@ _ref = None
 
 def build() -> None:
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
+
+
+def reference_dir() -> Path:
+    """The reference tree the recipes compile from: SMP_REFERENCE_DIR if set,
+    else the default of oracle/Makefile (its REF variable).  It exists only
+    where the reference is mounted; nothing on the GPU path reads it."""
+    env = os.environ.get("SMP_REFERENCE_DIR")
+    if env:
+        return Path(env)
+    out = subprocess.run(["make", "-s", "-C", str(HERE), "print-ref"], check=True, capture_output=True, text=True)
+    return Path(out.stdout.strip())
 
 
 def lib() -> ctypes.CDLL:

@@ -8,6 +8,7 @@ header is newer than the library.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -62,7 +63,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         return LIB
     nvcc = _nvcc()
     BUILD_DIR.mkdir(exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         obj = BUILD_DIR / (Path(src).stem + ".o")
         cmd = [nvcc, *ARCH_FLAGS, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(CSRC / src), "-o", str(obj)]
@@ -70,8 +71,15 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(str(obj))
+    # the translation units are independent: compile them side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+        for r in pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds):
+            sys.stdout.write(r.stdout)
+            sys.stderr.write(r.stderr)
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc, *ARCH_FLAGS, "-shared", "-o", str(tmp), *objs, "-Xcompiler", "-fPIC"]
     if verbose:
@@ -87,13 +95,19 @@ def build_oracle(verbose: bool = False) -> None:
     the studies time beside this library."""
     oracle = ROOT / "oracle"
     targets = ["all"]
-    ref = Path(os.environ.get("SMP_REFERENCE_DIR", "/root/reference"))
+    ref = os.environ.get("SMP_REFERENCE_DIR")
+    if not ref:  # the recipe's own default location of the reference tree
+        ref = subprocess.run(["make", "-s", "-C", str(oracle), "print-ref"], check=True, capture_output=True,
+                             text=True).stdout.strip()
+    ref = Path(ref)
     if (ref / "src" / "smp" / "smp_engine_gs_1.cu").exists():
         targets.append("ref")
     if (ref / "include" / "smp" / "smp_init_3.h").exists():
         targets.append("ref-gpu")
     if (ref / "src" / "smp" / "smp_engine_bamboo.cu").exists():
         targets.append("ref-bamboo")
+    if (ref / "benchmark" / "smp_engine_exec.h").exists() and LIB.exists():
+        targets.append("ref-exec")
     cmd = ["make", "-s", "-C", str(oracle), *targets, f"REF={ref}"]
     if verbose:
         print(" ".join(cmd), flush=True)

@@ -225,7 +225,10 @@ __global__ void __launch_bounds__(512, 2) k_batch(BatchInstance *__restrict__ ta
       batch_invert_slab(pref_w, slab, n, G, reinterpret_cast<uint16_t *>(smem_raw), bad, false);
       if (bad) s_status = SMP_ERR_INVALID_INPUT;
       __syncthreads();
-      for (int m = tid; m < n; m += blockDim.x) sbid[m] = 0xFFFFFFFFu;  // the men, holding no woman
+      for (int m = tid; m < n; m += blockDim.x) {
+        sbid[m] = 0xFFFFFFFFu;  // the men, holding no woman
+        spos[m] = 0;            // the women's positions (a racing relaxed read sees 0, never leftovers)
+      }
       __syncthreads();
       {
         // women propose down their lists; every man ranks a woman by her
@@ -273,7 +276,13 @@ __global__ void __launch_bounds__(512, 2) k_batch(BatchInstance *__restrict__ ta
       __syncthreads();
       continue;
     }
-    for (int w = tid; w < n; w += blockDim.x) sbid[w] = 0xFFFFFFFFu;
+    // Positions start at 0, so a relaxed read of a displaced man's position
+    // that races with his own store returns an earlier position (resuming
+    // there only repeats rejected proposals), never leftover shared memory.
+    for (int w = tid; w < n; w += blockDim.x) {
+      sbid[w] = 0xFFFFFFFFu;
+      spos[w] = 0;
+    }
     __syncthreads();
 
     // 1. inversion: through the shared region in groups of rows when the

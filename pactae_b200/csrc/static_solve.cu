@@ -83,7 +83,14 @@ __global__ void __launch_bounds__(1024, 1) k_solve_static(const int32_t *__restr
     s_next = 0;
     s_props = 0;
   }
-  for (int w = tid; w < n; w += blockDim.x) sbid[w] = 0xFFFFFFFFu;
+  // Positions start at 0: a relaxed read of a displaced man's position that
+  // races with his own store then returns 0 or an earlier position, never
+  // leftover shared memory from another kernel (resuming early only repeats
+  // proposals that are rejected again).
+  for (int w = tid; w < n; w += blockDim.x) {
+    sbid[w] = 0xFFFFFFFFu;
+    spos[w] = 0;
+  }
   __syncthreads();
 
   // 1. Inversion, one row per warp: scatter, then read back to check the row

@@ -157,3 +157,25 @@ def test_fixed_shape_is_kept(ctx):
                                   "rank_smem_kb": -1, "tune": -1}
         status, props, st = batch.run()
     assert st["failed"] == 0
+
+
+def test_batch_top_of_the_mix_against_oracle(ctx):
+    # The largest instances the mix draws (n in (2048, 4096]) of all three
+    # kinds: the grouped slab inversion and, for the congested ones, the
+    # women-proposing role swap, checked against the oracle's men-proposing
+    # Gale-Shapley; small instances ride along so both rank placements run.
+    import torch
+
+    sizes = [(pb.SMP_GEN_UNIFORM, 4096), (pb.SMP_GEN_CONGESTED, 4096), (pb.SMP_GEN_CORRELATED, 4096),
+             (pb.SMP_GEN_UNIFORM, 2049), (pb.SMP_GEN_CONGESTED, 3001), (pb.SMP_GEN_CORRELATED, 2600),
+             (pb.SMP_GEN_UNIFORM, 100), (pb.SMP_GEN_CORRELATED, 64)]
+    insts = []
+    for b, (kind, n) in enumerate(sizes):
+        pm, pw = ctx.generate(kind, n, seed=31, salt=b, param=KIND_PARAM[kind])
+        insts.append((pm, pw, torch.full((n,), -1, dtype=torch.int32, device=pm.device)))
+    with pb.Batch(ctx, insts) as batch:
+        status, props, st = batch.run()
+    assert st["failed"] == 0 and all(s == 0 for s in status)
+    for (pm, pw, mt), p in zip(insts, props):
+        want, wp = oracle.gs_seq(pm.cpu().numpy(), pw.cpu().numpy())
+        assert np.array_equal(mt.cpu().numpy(), want) and p == wp

@@ -102,3 +102,29 @@ def test_solves_beside_the_server(ctx):
             assert res["status"] == 0
             assert np.array_equal(mt.cpu().numpy(), want.cpu().numpy())
             assert res["proposals"] == wst["proposals"]
+
+
+def test_large_requests_up_to_16384(ctx):
+    # The top of the serving mix (n up to 16384, all three kinds) goes
+    # through the large-request route -- each on its own context and stream,
+    # several at once, beside a wave of small requests -- and every result
+    # must equal the same request solved alone.
+    import torch
+
+    sizes = [(pb.SMP_GEN_UNIFORM, 16384), (pb.SMP_GEN_CONGESTED, 12000), (pb.SMP_GEN_CORRELATED, 9000),
+             (pb.SMP_GEN_UNIFORM, 5003), (pb.SMP_GEN_CORRELATED, 16384), (pb.SMP_GEN_CONGESTED, 4097)]
+    reqs = []
+    for b, (kind, n) in enumerate(sizes):
+        pm, pw = ctx.generate(kind, n, seed=61, salt=b, param=KIND_PARAM[kind])
+        reqs.append((pm, pw, torch.full((n,), -1, dtype=torch.int32, device=pm.device)))
+    reqs += make_requests(ctx, 12, seed=62, n_lo=64, n_hi=900)
+    alone = [ctx.solve(pm, pw) for pm, pw, _ in reqs]
+    with pb.Server(large_slots=3) as srv:
+        tickets = [srv.submit(pm, pw, mt) for pm, pw, mt in reqs]
+        results = [srv.poll(t) for t in tickets]
+        st = srv.stats()
+    assert st["large"] >= len(sizes)
+    for (pm, pw, mt), (want, wst), res in zip(reqs, alone, results):
+        assert res["status"] == 0
+        assert np.array_equal(mt.cpu().numpy(), want.cpu().numpy())
+        assert res["proposals"] == wst["proposals"]

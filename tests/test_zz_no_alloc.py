@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -47,6 +48,17 @@ def test_static_solve_matches_regular_solve():
             assert rc == pb.SMP_OK, rc
             assert torch.equal(out, want), (kind, n)
             assert props.value == st["proposals"]
+
+        # one case pinned to the oracle itself, independently of smp_b200_solve
+        import oracle
+
+        pm, pw = ctx.generate(pb.SMP_GEN_CORRELATED, 999, seed=14, param=300)
+        want, props_want = oracle.gs_seq(pm.cpu().numpy(), pw.cpu().numpy())
+        out = torch.full((999,), -1, dtype=torch.int32, device="cuda:0")
+        props = ctypes.c_int64(-1)
+        torch.cuda.synchronize()
+        rc = lib.smp_b200_solve_static(_p(pm), _p(pw), 999, _p(out), ctypes.byref(props), None)
+        assert rc == pb.SMP_OK and np.array_equal(out.cpu().numpy(), want) and props.value == props_want
 
         # beyond the fixed array: refused before anything runs
         big = _lib.SMP_B200_STATIC_MAX_N + 1
