@@ -72,7 +72,8 @@ typedef enum smp_status {
   SMP_ERR_INVALID_INPUT = 2, /* a preference row is not a permutation       */
   SMP_ERR_OOM = 3,           /* device or pinned allocation failed          */
   SMP_ERR_CUDA = 4,          /* a CUDA call failed                          */
-  SMP_ERR_TIMEOUT = 5,       /* a bounded device wait ran out               */
+  SMP_ERR_TIMEOUT = 5,       /* reserved: no call waits on the device with a */
+                             /* time limit, so none returns it              */
   SMP_ERR_BUSY = 6,          /* serving: no slot or HBM budget free          */
   SMP_ERR_NOT_READY = 7,     /* serving: the ticket has not finished         */
   SMP_ERR_UNSUPPORTED = 8,   /* request outside this build's limits          */
@@ -112,7 +113,11 @@ typedef struct smp_cfg {
                            /* 0 = 64 GiB                                            */
   int32_t tail_window;     /* the same for the tail kernel; 0 = auto                */
   int32_t mode;            /* 0 = auto, 1 = the men's rank-matrix mode only         */
-  uint64_t reserved[3];
+  int32_t rank_bytes;      /* bytes per rank-matrix entry: 0 = auto (2 up to        */
+                           /* n = 65535, else 4), 4 = int32 ranks at any n (the     */
+                           /* layout every n above 65535 uses)                      */
+  int32_t reserved32;
+  uint64_t reserved[2];
 } smp_cfg;
 
 typedef struct smp_stats {
@@ -145,6 +150,10 @@ typedef struct smp_stats {
 SMP_B200_API int smp_b200_create(smp_ctx **out, const smp_cfg *cfg);
 SMP_B200_API void smp_b200_destroy(smp_ctx *ctx);
 SMP_B200_API const char *smp_b200_strerror(int status);
+/* The message of the context's last failed call (which step, and the CUDA
+ * error text where there is one); "" if none.  Valid until the next call on
+ * the context. */
+SMP_B200_API const char *smp_b200_last_error(const smp_ctx *ctx);
 SMP_B200_API const char *smp_b200_version(void);
 
 /* Phase API (AbsSmpEngine's template method, one call per phase). */

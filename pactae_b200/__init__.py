@@ -61,15 +61,18 @@ __all__ = ["Batch", "Server", "Context", "SmpError", "SmpObj", "SmpEngineB200", 
 class SmpError(RuntimeError):
     """A non-OK smp_status from the library."""
 
-    def __init__(self, status: int, where: str = ""):
+    def __init__(self, status: int, where: str = "", detail: str = ""):
         self.status = status
         msg = lib.smp_b200_strerror(status).decode()
+        if detail:
+            msg = f"{msg}: {detail}"
         super().__init__(f"{where}: {msg} (status {status})" if where else f"{msg} (status {status})")
 
 
-def _check(status: int, where: str) -> None:
+def _check(status: int, where: str, handle: Any = None) -> None:
     if status != SMP_OK:
-        raise SmpError(status, where)
+        detail = lib.smp_b200_last_error(handle).decode() if handle is not None else ""
+        raise SmpError(status, where, detail)
 
 
 def version() -> str:
@@ -96,7 +99,7 @@ class Context:
     buffers on one device.  Not thread-safe; use one per thread."""
 
     def __init__(self, device: int = 0, prefix_k: int = 0, tail_threshold: int = 0, hbm_budget: int = 0,
-                 bulk_window: int = 0, tail_window: int = 0, mode: int = 0):
+                 bulk_window: int = 0, tail_window: int = 0, mode: int = 0, rank_bytes: int = 0):
         cfg = smp_cfg()
         cfg.device = device
         cfg.prefix_k = prefix_k
@@ -105,6 +108,7 @@ class Context:
         cfg.bulk_window = bulk_window
         cfg.tail_window = tail_window
         cfg.mode = mode
+        cfg.rank_bytes = rank_bytes
         handle = ctypes.c_void_p()
         _check(lib.smp_b200_create(ctypes.byref(handle), ctypes.byref(cfg)), "smp_b200_create")
         self._h = handle
@@ -156,7 +160,7 @@ class Context:
             rc = lib.smp_b200_solve(self.handle, ctypes.c_void_p(pref_m.data_ptr()),
                                     ctypes.c_void_p(pref_w.data_ptr()), n, ctypes.c_void_p(match.data_ptr()),
                                     flags | SMP_F_DEVICE_PTRS, ctypes.byref(st))
-            _check(rc, "smp_b200_solve")
+            _check(rc, "smp_b200_solve", self.handle)
             return match, st.as_dict()
         pm = _host_array(pref_m)
         n = n or int(round(np.sqrt(pm.size)))
@@ -164,7 +168,7 @@ class Context:
         pw = _host_array(pref_w, n, "pref_w")
         match = out if out is not None else np.empty(n, dtype=np.int32)
         rc = lib.smp_b200_solve(self.handle, _ptr(pm), _ptr(pw), n, _ptr(match), flags, ctypes.byref(st))
-        _check(rc, "smp_b200_solve")
+        _check(rc, "smp_b200_solve", self.handle)
         return match, st.as_dict()
 
     # -- phases (AbsSmpEngine::FindStableMatching, smp_engine_abs.h:10-36) ---

@@ -45,6 +45,7 @@ ABI_SYMBOLS = (
     "smp_b200_create",
     "smp_b200_destroy",
     "smp_b200_strerror",
+    "smp_b200_last_error",
     "smp_b200_version",
     "smp_b200_stage",
     "smp_b200_precheck",
@@ -81,7 +82,9 @@ class smp_cfg(ctypes.Structure):
         ("hbm_budget", ctypes.c_uint64),
         ("tail_window", ctypes.c_int32),
         ("mode", ctypes.c_int32),
-        ("reserved", ctypes.c_uint64 * 3),
+        ("rank_bytes", ctypes.c_int32),
+        ("reserved32", ctypes.c_int32),
+        ("reserved", ctypes.c_uint64 * 2),
     ]
 
 
@@ -204,6 +207,7 @@ _SIGNATURES = {
     "smp_b200_create": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.POINTER(smp_cfg)]),
     "smp_b200_destroy": (None, [_P]),
     "smp_b200_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+    "smp_b200_last_error": (ctypes.c_char_p, [_P]),
     "smp_b200_version": (ctypes.c_char_p, []),
     "smp_b200_stage": (ctypes.c_int, [_P, _P, _P, _I32, _U32]),
     "smp_b200_precheck": (ctypes.c_int, [_P, ctypes.POINTER(_I32)]),

@@ -163,6 +163,7 @@ struct Ctx {
   int bulk_window_cfg = 0;
   int tail_window_cfg = 0;
   int mode_cfg = 0;
+  int rank_bytes_cfg = 0;  // 4: int32 ranks at any n
   uint64_t hbm_budget = 64ull << 30;
   std::string last_error;
 

@@ -2,6 +2,7 @@
 // solve, the whole-solve call, rank inversion, stability check and the
 // seeded generator.  Host code only orchestrates; the work is in
 // solve_kernels.cuh and generate.cu.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -101,7 +102,7 @@ int enqueue_validate(Ctx &c) {
 // the query mode may run, and the tail threshold.
 void plan(Ctx &c) {
   const int n = c.n;
-  c.rank_bytes = rank_bytes_for(n);
+  c.rank_bytes = c.rank_bytes_cfg == 4 ? 4 : rank_bytes_for(n);
   c.K = 0;
   if (c.rank_bytes == 2 && c.prefix_k_cfg >= 0) {
     const int want = c.prefix_k_cfg > 0 ? c.prefix_k_cfg : kDefaultPrefixK;
@@ -136,9 +137,9 @@ int enqueue_precheck(Ctx &c, bool allow_perfect) {
 template <typename RankT>
 int enqueue_invert(Ctx &c, const int32_t *pref_w, RankT *rank, int gate) {
   const int n = c.n;
+  const size_t smem16 = row_smem_bytes<uint16_t>(n);  // n <= 65535: at most 131 KB
   if constexpr (std::is_same<RankT, int32_t>::value) {
-    const size_t smem16 = row_smem_bytes<uint16_t>(n);
-    if (n <= kU16MaxN && smem16 <= c.smem_optin) {  // int32 output from a uint16 shared row
+    if (n <= kU16MaxN) {  // int32 output from a uint16 shared row
       if (allow_dynamic_smem(c, k_invert_wide) != cudaSuccess)
         return c.fail_cuda("k_invert_wide smem attribute");
       int per_sm = 0;
@@ -151,30 +152,27 @@ int enqueue_invert(Ctx &c, const int32_t *pref_w, RankT *rank, int gate) {
       c.launches++;
       return c.check_launch("k_invert_wide");
     }
-  }
-  const size_t smem = row_smem_bytes<RankT>(n);
-  if (smem <= c.smem_optin) {
-    if (allow_dynamic_smem(c, k_invert<RankT>) != cudaSuccess)
-      return c.fail_cuda("k_invert smem attribute");
+    // Rows of more than 65535 ranks do not fit a shared row: scatter straight
+    // to global memory, then verify.
+    k_invert_global<<<c.sm_count * 8, 256, 0, c.stream>>>(pref_w, rank, n, c.d_ctrl.as<Control>(), gate);
+    c.launches++;
+    int rc = c.check_launch("k_invert_global");
+    if (rc) return rc;
+    k_invert_verify<<<c.sm_count * 8, 256, 0, c.stream>>>(pref_w, rank, n, c.d_ctrl.as<Control>(), gate);
+    c.launches++;
+    return c.check_launch("k_invert_verify");
+  } else {
+    if (allow_dynamic_smem(c, k_invert<RankT>) != cudaSuccess) return c.fail_cuda("k_invert smem attribute");
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_invert<RankT>, 512, smem) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_invert<RankT>, 512, smem16) != cudaSuccess) {
       cudaGetLastError();
       per_sm = 1;
     }
     const int grid = std::min(n, c.sm_count * std::max(per_sm, 1));
-    k_invert<RankT><<<grid, 512, smem, c.stream>>>(pref_w, rank, n, c.d_ctrl.as<Control>(), gate);
+    k_invert<RankT><<<grid, 512, smem16, c.stream>>>(pref_w, rank, n, c.d_ctrl.as<Control>(), gate);
     c.launches++;
     return c.check_launch("k_invert");
   }
-  // Rows too long for shared memory (int32 ranks only).
-  int32_t *r32 = reinterpret_cast<int32_t *>(rank);
-  k_invert_global<<<c.sm_count * 8, 256, 0, c.stream>>>(pref_w, r32, n, c.d_ctrl.as<Control>(), gate);
-  c.launches++;
-  int rc = c.check_launch("k_invert_global");
-  if (rc) return rc;
-  k_invert_verify<<<c.sm_count * 8, 256, 0, c.stream>>>(pref_w, r32, n, c.d_ctrl.as<Control>(), gate);
-  c.launches++;
-  return c.check_launch("k_invert_verify");
 }
 
 int enqueue_invert_any(Ctx &c, int gate) {
@@ -224,17 +222,6 @@ int enqueue_rank(Ctx &c, int gate) {
 template <typename RankT>
 const RankT *proposal_ranks(const Ctx &c) {
   return reinterpret_cast<const RankT *>(rank_layout<RankT>() == 2 ? c.d_pr.ptr : c.d_rankT.ptr);
-}
-
-int enqueue_prefix_gather(Ctx &c, int gate) {
-  if (c.K <= 0 || c.rank_bytes == 2) return SMP_OK;  // uint16 ranks: k_pr wrote the prefix
-  const int n = c.n;
-  const size_t total = static_cast<size_t>(n) * c.K;
-  const int grid = static_cast<int>(std::min<size_t>(static_cast<size_t>(c.sm_count) * 16, (total + 255) / 256));
-  k_prefix<<<grid, 256, 0, c.stream>>>(c.pref_m, c.d_rankT.as<uint16_t>(), c.d_prefix.as<uint32_t>(), n, c.K,
-                                       c.d_ctrl.as<Control>(), gate);
-  c.launches++;
-  return c.check_launch("k_prefix");
 }
 
 // Query mode: bucket the (man, position) pairs of every man's first K
@@ -325,8 +312,9 @@ int enqueue_init(Ctx &c) {
   }
   if (c.known_mode != kModeQuery) rc = enqueue_rank(c, kGateModeRank);
   if (rc) return rc;
+  // (k_pr wrote the prefix beside the uint16 ranks; int32 ranks run without one)
   if (cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
-  return c.known_mode == kModeQuery ? SMP_OK : enqueue_prefix_gather(c, kGateModeRank);
+  return SMP_OK;
 }
 
 template <typename RankT, int kSub>
@@ -435,7 +423,6 @@ int enqueue_retry_round(Ctx &c) {
   c.launches++;
   int rc = c.check_launch("k_retry_reset");
   if (!rc) rc = enqueue_rank(c, kGateRetry);
-  if (!rc) rc = enqueue_prefix_gather(c, kGateRetry);
   if (!rc) rc = enqueue_round<RankT>(c, 1);
   return rc;
 }
@@ -691,7 +678,7 @@ int solve_enqueue(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t 
 // keep their gates, so the device still decides what runs.  The checker
 // (SMP_F_CHECK) must see the final matching: those solves take the fully
 // gated pipeline.
-int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped);
+int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped, bool men_screened = false);
 
 int solve_staged(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
                  uint32_t flags, smp_stats *st) {
@@ -761,7 +748,7 @@ int solve_staged(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n
 // rows are permutations); if so, the women propose and `swapped` is set,
 // else the caller runs the men's rank-mode pass.  Stops after the screen,
 // with `swapped` set, when it found invalid input.
-int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped) {
+int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped, bool men_screened) {
   swapped = false;
   const int n = c.n;
   const size_t screen_smem = swap_screen_smem(n);
@@ -783,8 +770,9 @@ int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped) {
     cudaGetLastError();
     per_sm = 1;
   }
-  k_swap_screen<<<std::min(2 * n, c.sm_count * std::max(per_sm, 1)), 256, screen_smem, c.stream>>>(
-      c.pref_m, c.pref_w, n, ctrl);
+  const int t0 = men_screened ? n : 1;  // the host compared the men's rows already
+  k_swap_screen<<<std::max(1, std::min(2 * n - t0, c.sm_count * std::max(per_sm, 1))), 256, screen_smem, c.stream>>>(
+      c.pref_m, c.pref_w, n, ctrl, t0);
   c.launches += 2;
   rc = c.check_launch("k_swap_screen");
   if (!rc && cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
@@ -901,6 +889,27 @@ void pack_rows(Ctx &c, const int32_t *src, uint16_t *dst, size_t count, int n) {
   c.pack_pool->run(job);
 }
 
+// Does every row of the host matrix pref_m equal row 0?  Rows are compared
+// on the context's host threads, which stop at the first difference.
+bool host_rows_equal_row0(Ctx &c, const int32_t *pref_m, int n) {
+  if (!c.pack_pool) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    c.pack_pool.reset(new (std::nothrow) HostPool(static_cast<int>(std::min(hw, 12u))));
+    if (!c.pack_pool) return false;
+  }
+  std::atomic<bool> differ{false};
+  const size_t row_bytes = sizeof(int32_t) * static_cast<size_t>(n);
+  const auto job = [&](int i, int parts) {
+    const int r0 = 1 + static_cast<int>(static_cast<int64_t>(n - 1) * i / parts);
+    const int r1 = 1 + static_cast<int>(static_cast<int64_t>(n - 1) * (i + 1) / parts);
+    for (int r = r0; r < r1 && !differ.load(std::memory_order_relaxed); ++r)
+      if (std::memcmp(pref_m + static_cast<size_t>(r) * n, pref_m, row_bytes) != 0)
+        differ.store(true, std::memory_order_relaxed);
+  };
+  c.pack_pool->run(job);
+  return !differ.load();
+}
+
 int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
                    uint32_t flags, smp_stats *st) {
   const size_t row = sizeof(int32_t) * static_cast<size_t>(n);
@@ -941,15 +950,26 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
   if (!c.h_ctrl->perfect) c.known_mode = c.h_ctrl->mode;  // enqueue only this mode's kernels
   bool swapped = false;
   if (!query) {
+    // One first choice for every man: perhaps one list for every man.  Then
+    // the host threads compare every man's row with row 0 while pref_w
+    // crosses the link, and only row 0 of pref_m follows it: the
+    // women-proposing pass reads nothing else of it.
+    const bool try_shared = !c.h_ctrl->perfect && c.h_ctrl->mode == kModeRank && c.h_ctrl->distinct == 1 &&
+                            c.mode_cfg == 0 && swap_screen_smem(n) <= c.smem_optin;
+    bool shared = false;
     if (!c.h_ctrl->perfect) {
-      rc = copy_rest_of_m();
-      if (!rc && cudaMemcpyAsync(dw, pref_w, row * n, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+      if (cudaMemcpyAsync(dw, pref_w, row * n, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
         rc = c.fail_cuda("pref_w copy");
+      if (!rc && try_shared) {
+        if (cudaMemcpyAsync(dm + c.K, pref_m + c.K, sizeof(int32_t) * (n - c.K), cudaMemcpyHostToDevice, c.stream) !=
+            cudaSuccess)
+          rc = c.fail_cuda("pref_m row 0 copy");
+        if (!rc) shared = host_rows_equal_row0(c, pref_m, n);
+      }
+      if (!rc && !shared) rc = copy_rest_of_m();
     }
     if (!rc && cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-    // one first choice for every man: perhaps one list for every man
-    if (!rc && !c.h_ctrl->perfect && c.h_ctrl->mode == kModeRank && c.h_ctrl->distinct == 1 && c.mode_cfg == 0)
-      rc = solve_swapped(c, flags, match_out, swapped);
+    if (!rc && shared) rc = solve_swapped(c, flags, match_out, swapped, true);
     if (!rc && !swapped) rc = enqueue_init(c);
     if (!rc && !swapped && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
     if (!rc && !swapped) rc = enqueue_core(c);
@@ -1040,7 +1060,7 @@ const char *smp_b200_strerror(int status) {
     case SMP_ERR_INVALID_INPUT: return "invalid input: a preference row is not a permutation of 0..n-1";
     case SMP_ERR_OOM: return "out of device or pinned memory";
     case SMP_ERR_CUDA: return "CUDA error";
-    case SMP_ERR_TIMEOUT: return "a bounded device wait timed out";
+    case SMP_ERR_TIMEOUT: return "timed out (reserved: no call returns it)";
     case SMP_ERR_BUSY: return "no slot or HBM budget free";
     case SMP_ERR_NOT_READY: return "not finished yet";
     case SMP_ERR_UNSUPPORTED: return "unsupported request";
@@ -1048,6 +1068,8 @@ const char *smp_b200_strerror(int status) {
     default: return "unknown status";
   }
 }
+
+const char *smp_b200_last_error(const smp_ctx *ctx) { return ctx ? ctx->c.last_error.c_str() : ""; }
 
 int smp_b200_create(smp_ctx **out, const smp_cfg *cfg) {
   if (!out) return SMP_ERR_INVALID_ARG;
@@ -1062,7 +1084,12 @@ int smp_b200_create(smp_ctx **out, const smp_cfg *cfg) {
     c.bulk_window_cfg = cfg->bulk_window;
     c.tail_window_cfg = cfg->tail_window;
     c.mode_cfg = cfg->mode;
+    c.rank_bytes_cfg = cfg->rank_bytes;
     if (cfg->hbm_budget) c.hbm_budget = cfg->hbm_budget;
+    if (cfg->rank_bytes != 0 && cfg->rank_bytes != 4) {
+      delete ctx;
+      return SMP_ERR_INVALID_ARG;
+    }
   }
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || c.device < 0 || c.device >= count) {
@@ -1298,7 +1325,7 @@ int smp_b200_check(smp_ctx *ctx, const int32_t *pref_m, const int32_t *pref_w, i
   }
   rc = enqueue_precheck(c, false);
   if (rc) return rc;
-  c.rank_bytes = rank_bytes_for(n);
+  c.rank_bytes = c.rank_bytes_cfg == 4 ? 4 : rank_bytes_for(n);
   rc = c.d_rank.ensure(static_cast<size_t>(n) * n * c.rank_bytes);
   if (rc) return rc;
   if (cudaEventRecord(c.ev[kEvCheckBegin], c.stream) != cudaSuccess) return c.fail_cuda("event");

@@ -4,9 +4,9 @@
 //                                                          include/smp/smp_engine_bamboo.h:25-33)
 //   k_invert      rank[w][pref_w[w][r]] = r              (F9RankMatrixInitKernel,
 //                                                          src/smp/kernel.cu:672-686)
-//   k_prefix      per-man (woman, rank) pairs for the first K choices, gathered
-//                 from the rank matrix: the part of the reference's PR matrix
-//                 (kernel.cu:688-709) that a solve reads
+//   k_pr          ranks by position, pr[m][r] = rank of m in his r-th choice's
+//                 list, and each man's first K (woman, rank) pairs: the
+//                 reference's PR matrix (kernel.cu:688-709) in uint16
 //   k_q*          the same prefix answered straight from pref_w rows, without
 //                 a rank matrix (query mode)
 //   k_bulk        proposals on every SM                  (La3F9CoreKernel, kernel.cu:633-670)
@@ -414,31 +414,6 @@ __global__ void __launch_bounds__(512) k_validate_rows(const int32_t *__restrict
 }
 
 // ---------------------------------------------------------------------------
-// Prefix gather (rank mode): prefix[m][r] = w << 16 | rankT[m][w] for
-// w = pref_m[m][r], r < K, from the man-major rank matrix (a man's entries
-// come from his own row).  An out-of-range woman is reported and her entry
-// set to 0xFFFFFFFF.
-// ---------------------------------------------------------------------------
-__global__ void k_prefix(const int32_t *__restrict__ pref_m, const uint16_t *__restrict__ rankT,
-                         uint32_t *__restrict__ prefix, int n, int K, Control *ctrl, int gate) {
-  if (!gate_open(gate, ctrl)) return;
-  const size_t total = static_cast<size_t>(n) * K;
-  const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
-  for (size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += stride) {
-    const int m = static_cast<int>(t / K);
-    const int r = static_cast<int>(t - static_cast<size_t>(m) * K);
-    const int w = __ldg(pref_m + static_cast<size_t>(m) * n + r);
-    uint32_t e = 0xFFFFFFFFu;
-    if (static_cast<unsigned>(w) < static_cast<unsigned>(n)) {
-      e = (static_cast<uint32_t>(w) << 16) | __ldg(rankT + static_cast<size_t>(m) * n + w);
-    } else {
-      report(ctrl, kStatusInvalidInput, w);
-    }
-    prefix[t] = e;
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Query mode.  The prefix needs rank_w(m) only for the n*K pairs (w, m) with
 // w among m's first K choices.  k_qscatter buckets those pairs by woman into
 // fixed-capacity buckets (qlist[w * qcap + i], qcnt[w] of them): qcap =
@@ -653,8 +628,7 @@ __host__ __device__ constexpr int rank_layout() {
 // instead of a random rankT[m][w] that waits for pref_m[m][r]; in congested
 // and correlated lists, where men reject hundreds of women per acceptance,
 // that halves the round trips of a window.  The same pass writes each man's
-// first K entries of the prefix table (woman << 16 | rank, as k_prefix
-// would).  One CTA per man row at a time:
+// first K entries of the prefix table (woman << 16 | rank).  One CTA per man row at a time:
 // his rankT row is staged in shared memory (16-byte loads over its aligned
 // interior), his pref_m row streams in with 16-byte loads and gathers from
 // it.  An out-of-range woman is reported.
@@ -680,7 +654,7 @@ __global__ void __launch_bounds__(512) k_pr(const int32_t *__restrict__ pref_m, 
     __syncthreads();
     const RowSpan s = row_span(pref_m, m, n);
     uint16_t *out = pr + static_cast<size_t>(m) * n;
-    uint32_t *pfx = prefix + static_cast<size_t>(m) * K;  // his first K choices, packed as k_prefix does
+    uint32_t *pfx = prefix + static_cast<size_t>(m) * K;  // his first K choices, woman << 16 | rank
     const auto gather = [&](int w, int r) {
       if (static_cast<unsigned>(w) < static_cast<unsigned>(n)) {
         out[r] = srow[w];
@@ -971,9 +945,13 @@ __host__ __device__ constexpr size_t tail_smem_bytes(int n) {
 }
 
 // The global bid words as shared ones (rank << 16 | man) plus each matched
-// man's position.  The caller synchronises.
+// man's position; every other position starts at 0, so a relaxed read that
+// races with a man's first store returns 0 (an earlier position), never
+// leftover shared memory.  Called by the whole CTA; the caller synchronises.
 __device__ __forceinline__ void tail_setup(const unsigned long long *__restrict__ bid, uint32_t *sbid,
                                            uint16_t *spos, int n) {
+  for (int m = threadIdx.x; m < n; m += blockDim.x) spos[m] = 0;
+  __syncthreads();
   for (int w = threadIdx.x; w < n; w += blockDim.x) {
     const unsigned long long b = bid[w];
     if (b == kFree) {

@@ -35,7 +35,9 @@ __global__ void k_swap_pos(const int32_t *__restrict__ pref_m, int32_t *__restri
 }
 
 // Rows t = 1 .. n-1 compare pref_m row t with row 0; rows t = n .. 2n-1
-// check that pref_w row t-n is a permutation with a shared bitmap.  Row
+// check that pref_w row t-n is a permutation with a shared bitmap.  A solve
+// whose men's rows were compared on the host (host-input solves) starts at
+// t0 = n: only row 0 of pref_m is then on the device.  Row
 // bodies move in 16-byte loads (row_span: rows start off 16-byte boundaries
 // when n is not a multiple of 4).  Once a pref_m row differs, the solve
 // takes the men's rank-mode pass, which checks pref_w itself: the CTAs stop.
@@ -44,7 +46,8 @@ __global__ void k_swap_pos(const int32_t *__restrict__ pref_m, int32_t *__restri
 __host__ __device__ constexpr size_t swap_screen_smem(int n) { return ((static_cast<size_t>(n) + 31) / 32) * 4; }
 
 __global__ void __launch_bounds__(256) k_swap_screen(const int32_t *__restrict__ pref_m,
-                                                     const int32_t *__restrict__ pref_w, int n, Control *ctrl) {
+                                                     const int32_t *__restrict__ pref_w, int n, Control *ctrl,
+                                                     int t0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   uint32_t *seen = reinterpret_cast<uint32_t *>(smem_raw);
   __shared__ int s_stop;
@@ -54,7 +57,7 @@ __global__ void __launch_bounds__(256) k_swap_screen(const int32_t *__restrict__
   const int words = (n + 31) >> 5;
   bool bad = false;
   int bad_value = 0;
-  for (int t = 1 + static_cast<int>(blockIdx.x); t < 2 * n; t += gridDim.x) {
+  for (int t = t0 + static_cast<int>(blockIdx.x); t < 2 * n; t += gridDim.x) {
     if (tid == 0) {
       s_stop = ld_volatile_s32(&ctrl->swap_fail) || ld_volatile_s32(&ctrl->status);
       s_wsame = !ld_volatile_s32(&ctrl->w_differ);

@@ -394,3 +394,95 @@ def test_query_bucket_overflow_falls_back_to_rank_mode():
         match, st = c.solve(pm, pw)
     assert np.array_equal(match, want) and st["proposals"] == props
     assert st["mode"] == 2  # query round abandoned, rank-mode round solved it
+
+
+# -- int32 ranks (the layout every n above 65535 uses), forced at small n ------
+@pytest.mark.parametrize("tail", [0, -1])
+def test_int32_ranks_match_reference(tail):
+    # rank_bytes = 4 runs the int32 template family -- the int32 inversion,
+    # transpose, bulk, tail (and its CTA-wide hand-over) and checker -- that
+    # sizes above 65535 take; with the tail off the matching comes from the
+    # bid words (k_match), as it does above 65535.
+    names = {"uniform_n2000", "congested_n2000", "correlated_n2000", "grouped5_n300", "solo_n1000",
+             "refcongested_n200", "uniform_n33", "uniform_n1", "perfect_n1000"}
+    with pb.Context(rank_bytes=4, tail_threshold=tail) as c:
+        for case in [x for x in SMALL if x["name"] in names]:
+            pm, pw = oracle.generate(case["kind"], case["n"], case["seed"], case["salt"], case["param"])
+            match, st = c.solve(pm, pw, check=True)
+            assert np.array_equal(match, golden_match(case["name"])), case["name"]
+            assert st["proposals"] == case["proposals"] and st["blocking_pairs"] == 0
+            if not st["perfect"] and st["mode"] != 3:
+                assert st["rank_bytes"] == 4
+        # device inputs and the inversion entry point too
+        case = next(x for x in SMALL if x["name"] == "correlated_n500")
+        pm, pw = c.generate(case["kind"], case["n"], case["seed"], case["salt"], case["param"])
+        match, st = c.solve(pm, pw)
+        assert np.array_equal(to_host(match), golden_match(case["name"])) and st["rank_bytes"] == 4
+        assert np.array_equal(c.invert(to_host(pw)), oracle.invert(to_host(pw)))
+
+
+def test_rank_bytes_knob_rejects_other_widths():
+    with pytest.raises(pb.SmpError) as e:
+        pb.Context(rank_bytes=2 + 1)
+    assert e.value.status == pb.SMP_ERR_INVALID_ARG
+
+
+def test_error_text_names_the_failure(ctx):
+    pm, pw = oracle.generate(pb.SMP_GEN_UNIFORM, 50, 3)
+    bad = pw.copy()
+    bad[4, 2] = bad[4, 3]
+    with pytest.raises(pb.SmpError) as e:
+        ctx.solve(pm, bad)
+    assert e.value.status == pb.SMP_ERR_INVALID_INPUT and "invalid input detected on the device" in str(e.value)
+
+
+@pytest.mark.slow
+def test_n_above_65535_uses_int32_ranks():
+    # n = 65600: rows of more than 65535 ranks, inverted straight in global
+    # memory and verified (k_invert_global / k_invert_verify), int32 ranks
+    # throughout, no tail kernel.  Device inputs ~17 GB per matrix; the
+    # oracle runs on the host copy when the host has room for it.
+    import psutil
+    import torch
+
+    n = 65600
+    nn = n * n
+    if psutil.virtual_memory().available < 6 * nn * 4:
+        pytest.skip("host memory too small for the oracle at n = 65600")
+    with pb.Context() as c:
+        pm, pw = c.generate(pb.SMP_GEN_UNIFORM, n, seed=21)
+        match, st = c.solve(pm, pw, check=True)
+        assert st["rank_bytes"] == 4 and st["blocking_pairs"] == 0
+        got = to_host(match)
+        hpm, hpw = to_host(pm), to_host(pw)
+        del pm, pw
+    torch.cuda.empty_cache()
+    want, props = oracle.gs_seq(hpm, hpw)
+    assert np.array_equal(got, want) and st["proposals"] == props
+
+
+@pytest.mark.parametrize("case", ["shared", "twisted", "both_shared", "bad_woman_row", "bad_shared_entry"])
+def test_host_input_men_sharing_one_list(case):
+    # Host-input solves of n >= 4096 whose men all make the same first choice
+    # compare the men's rows on the host while pref_w crosses the link; when
+    # they are all equal only row 0 of pref_m is sent and the women propose.
+    n = 4099
+    kind = pb.SMP_GEN_REF_CONGESTED if case == "both_shared" else pb.SMP_GEN_CONGESTED
+    pm, pw = oracle.generate(kind, n, 23)
+    pm, pw = pm.copy(), pw.copy()
+    if case == "twisted":
+        pm = twist(pm)
+    elif case == "bad_woman_row":
+        pw[n - 7, 11] = pw[n - 7, 12]
+    elif case == "bad_shared_entry":
+        pm[:, 40] = pm[:, 41]  # the shared list itself is not a permutation
+    with pb.Context() as c:
+        if case.startswith("bad"):
+            with pytest.raises(pb.SmpError) as e:
+                c.solve(pm, pw)
+            assert e.value.status == pb.SMP_ERR_INVALID_INPUT
+            return
+        match, st = c.solve(pm, pw)
+    want, props = oracle.gs_seq(pm, pw)
+    assert np.array_equal(match, want) and st["proposals"] == props
+    assert st["mode"] == (0 if case == "twisted" else 3)
