@@ -66,8 +66,14 @@ def parse_args():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     ap.add_argument("--batch-count", type=int, default=8192)
     ap.add_argument("--no-plain", action="store_true", help="skip the one-launch-per-instance baseline")
-    ap.add_argument("--serving-loads", default="0.3,0.7,1.0",
-                    help="offered loads as fractions of the measured saturation (e.g. 0.1,0.2,...,1.0)")
+    ap.add_argument("--serving-loads", default="0.1,0.2,0.3,0.4,0.5,0.6,0.7,0.8,0.9,1.0",
+                    help="offered loads as fractions of the measured saturation")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations (n=2000 on the reference CPU path, congested and "
+                         "correlated n=30000, Gs-Seq at n=30000)")
+    ap.add_argument("--no-bamboo", action="store_true", help="skip the reference GPU engine beside ours")
+    ap.add_argument("--no-solve-loop", action="store_true",
+                    help="skip the batch's one-smp_b200_solve-per-instance comparison")
     ap.add_argument("--serving-requests", type=int, default=150)
     return ap.parse_args()
 
@@ -394,6 +400,18 @@ def run_b200(args, dist: Dist) -> dict | None:
     # CPU baseline: the reference's Mw-Par-Cpu on the same instance, rank 0, N = 1
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline and result is not None:
         result["cpu_baseline"] = cpu_baseline(args, h_pm, h_pw, match.cpu().numpy(), ctx)
+    try:
+        del pm, pw
+    except NameError:
+        pass
+    torch.cuda.empty_cache()
+    # the other configurations and the reference's sequential engine, rank 0 at N = 1
+    if dist.rank == 0 and dist.world == 1 and not args.no_configs and result is not None and args.kind == 0:
+        result["configs"] = run_configs(ctx, args, h_pm, h_pw, match.cpu().numpy())
+        torch.cuda.empty_cache()
+    if dist.rank == 0 and dist.world == 1 and not args.no_bamboo and result is not None and args.kind == 0:
+        result["reference_gpu_engine"] = bamboo_cases(ctx, [(0, 2000, 1), (0, args.n, SEED)])
+        torch.cuda.empty_cache()
     del h_pm, h_pw
     torch.cuda.empty_cache()
     if not args.no_batch:
@@ -450,31 +468,68 @@ def run_batched(ctx, args, dist: Dist) -> dict:
         for _ in range(3):
             status, props, st = batch.run()
             runs.append(st)
+        assert all(x == 0 for x in status), "a batched instance failed"
         best = dist.max(min(r["ms"] for r in runs))  # best of 3 per rank, max over ranks
-        # the same roofline as a single solve, summed over the instances
-        b_alg = 8 * total + 36 * runs[-1]["proposals"]
+        # The same roofline as a single solve, summed over the instances,
+        # counting only proposals that are made: an instance whose men share
+        # one list (the congested third) is solved with the women proposing,
+        # so its men's n(n+1)/2 proposals are counted, not made, and its bytes
+        # are both lists read once (8 n^2), as for a single solve.
+        made = sum(p for p, (_, kind) in zip(props, metas) if kind != 1)
+        b_alg = 8 * total + 36 * made
         peak, _ = measured_peak_hbm()
         ach = b_alg / (best * 1e-3) / 1e9
+        inv = 8 * total / (best * 1e-3) / 1e9
         out["roofline"] = {"bound": "hbm", "algorithmic_bytes": b_alg, "achieved": round(ach, 1), "peak": peak,
                            "unit": "GB/s", "frac": round(ach / peak, 4),
-                           "formula": "sum over instances of 8 n^2 + 36 P, over the batched launch time"}
+                           "formula": "sum over instances of 8 n^2, plus 36 P for instances whose proposals are "
+                                      "made (not the women-proposing ones), over the batched launch time",
+                           "inversion_only_gbs": round(inv, 1), "inversion_only_frac": round(inv / peak, 4)}
         out.update({"batched_ms": round(best, 3), "batched_ms_runs": [round(r["ms"], 3) for r in runs],
                     "instances_per_s": round(count * dist.world / (best * 1e-3), 1),
                     "proposals": runs[-1]["proposals"], "failed": runs[-1]["failed"],
                     "launches_per_run": runs[-1]["launches"]})
-        # spot parity: a sample of instances against the single-instance solve
-        for b in range(0, count, max(1, count // 16)):
+        # spot parity: a sample of instances (the largest first) against the
+        # oracle's Gale-Shapley on the host
+        import numpy as np
+
+        import oracle
+
+        order = sorted(range(count), key=lambda b: -metas[b][0])
+        sample = order[:4] + [order[i] for i in range(4, count, max(1, count // 12))]
+        for b in sample:
             pm, pw, mt = insts[b]
             n = mt.numel()
-            want, _ = ctx.solve(pm.view(n, n), pw.view(n, n))
-            assert torch.equal(mt, want), f"batched instance {b} differs from its single solve"
+            want, wp = oracle.gs_seq(pm.view(n, n).cpu().numpy(), pw.view(n, n).cpu().numpy())
+            assert np.array_equal(mt.cpu().numpy(), want) and props[b] == wp, f"batched instance {b} differs"
+        out["oracle_checked"] = len(sample)
         if not args.no_plain:
             _, pprops, pst = batch.run_plain()
             assert pst["proposals"] == runs[-1]["proposals"] and pst["failed"] == 0
             out.update({"plain_ms": round(pst["ms"], 1),
                         "plain_instances_per_s": round(count / (pst["ms"] * 1e-3), 1),
                         "plain_launches": pst["launches"],
+                        "plain_note": "the same kernel launched once per instance with a grid of one CTA",
                         "batched_vs_plain": round(pst["ms"] / best, 1)})
+    if not args.no_solve_loop:
+        # The realistic per-instance alternative: every instance through the
+        # all-SM single-instance solve (smp_b200_solve, device pointers), one
+        # call after another; wall clock around the loop and the solves' own
+        # device time.
+        for pm, pw, mt in insts[:8]:  # warm the buffers for every size class
+            ctx.solve(pm.view(mt.numel(), -1), pw.view(mt.numel(), -1), out=mt)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dev_ms = 0.0
+        for pm, pw, mt in insts:
+            n = mt.numel()
+            _, st = ctx.solve(pm.view(n, n), pw.view(n, n), out=mt)
+            dev_ms += st["total_ms"]
+        loop_s = time.perf_counter() - t0
+        out.update({"solve_loop_s": round(loop_s, 3), "solve_loop_device_ms": round(dev_ms, 1),
+                    "solve_loop_instances_per_s": round(count / loop_s, 1),
+                    "batched_vs_solve_loop": round(loop_s * 1e3 / out["batched_ms"], 1),
+                    "solve_loop_note": "one smp_b200_solve call per instance (all SMs each), host wall clock"})
     del pool_m, pool_w, match, insts
     return out
 
@@ -498,6 +553,9 @@ def run_serving(ctx, args, dist: Dist) -> dict:
         n, kind = pb.batch_instance(6, b, 64, 16384)
         pm, pw = ctx.generate(kind, n, seed=6, salt=b, param=KIND_PARAM[kind])
         pool.append((pm, pw, n))
+    # each pool instance solved alone: every served matching must equal it
+    solo = [ctx.solve(pm, pw)[0].clone() for pm, pw, _ in pool]
+    checked = [0]
     rng = np.random.default_rng(6)
 
     def one_load(srv, rate, count):
@@ -527,6 +585,9 @@ def run_serving(ctx, args, dist: Dist) -> dict:
         wall = time.perf_counter() - t0
         lat = np.array([r["latency_ms"] for r in results])
         assert all(r["status"] == 0 for r in results)
+        for k, i in enumerate(picks):
+            assert torch.equal(outs[k], solo[i]), f"served request {k} differs from its instance solved alone"
+        checked[0] += count
         return {"offered_per_s": round(rate, 1) if rate else None, "requests": count,
                 "solves_per_s": round(count / wall, 1), "p50_ms": round(float(np.percentile(lat, 50)), 3),
                 "p99_ms": round(float(np.percentile(lat, 99)), 3), "mean_n": int(np.mean([pool[i][2] for i in picks]))}
@@ -545,7 +606,96 @@ def run_serving(ctx, args, dist: Dist) -> dict:
                         "uniform/congested/correlated, pool of 48 instances resident in HBM, "
                         "64 GiB admission budget", "saturation_solves_per_s": saturation,
             "burst": sat, "loads": loads, "waves": st["waves"], "large_path": st["large"],
-            "peak_admitted_gb": round(st["peak_bytes"] / 1e9, 2)}
+            "peak_admitted_gb": round(st["peak_bytes"] / 1e9, 2), "matchings_checked": checked[0]}
+
+
+def config_roofline(n: int, st: dict, ms: float) -> dict:
+    """The single-solve roofline (8 n^2 + 36 P, or 8 n^2 when the women
+    propose) for a solve of `ms` device milliseconds."""
+    peak, kind = measured_peak_hbm()
+    b = 8 * n * n if st["mode"] == 3 else 8 * n * n + 36 * st["proposals"]
+    ach = b / (ms * 1e-3) / 1e9
+    return {"algorithmic_bytes": b, "achieved_gbs": round(ach, 1), "peak": peak, "frac": round(ach / peak, 4),
+            "peak_source": kind}
+
+
+def run_configs(ctx, args, c2_pm, c2_pw, c2_match) -> dict:
+    """The configurations besides the headline one, each with the reference's
+    own CPU engines on the host cores: n = 2000 uniform (seed 1), the CPU
+    config, with Gs-Seq-CPU and Mw-Par-Cpu; congested (men share one list,
+    seed 3) and correlated (sigma = 0.05, seed 4) at n = 30000, device time
+    with the L2 flushed, phases, the host-input solve through the C ABI, and
+    Mw-Par-Cpu; and Gs-Seq-CPU on the headline instance.  Every matching is
+    checked against the reference engine's."""
+    import numpy as np
+    import torch
+
+    import oracle
+    import pactae_b200 as pb
+
+    out = {}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    have_ref = oracle.ref_available()
+    cases = [("n2000_uniform", pb.SMP_GEN_UNIFORM, 2000, 1, 0, 20),
+             ("n30000_congested", pb.SMP_GEN_CONGESTED, args.n, 3, 0, 5),
+             ("n30000_correlated", pb.SMP_GEN_CORRELATED, args.n, 4, 500, 5)]
+    for name, kind, n, seed, param, reps in cases:
+        pm, pw = ctx.generate(kind, n, seed=seed, param=param)
+        m = torch.empty(n, dtype=torch.int32, device=pm.device)
+        for _ in range(2):
+            ctx.solve(pm, pw, out=m)
+        dev = []
+        for _ in range(reps):
+            flush.random_(0, 255)
+            torch.cuda.synchronize()
+            _, st = ctx.solve(pm, pw, out=m)
+            dev.append(st)
+        best = min(dev, key=lambda x: x["total_ms"])
+        got = m.cpu().numpy()
+        hpm_t = torch.empty((n, n), dtype=torch.int32, pin_memory=True)
+        hpw_t = torch.empty((n, n), dtype=torch.int32, pin_memory=True)
+        hpm_t.copy_(pm)
+        hpw_t.copy_(pw)
+        del pm, pw, m
+        torch.cuda.empty_cache()
+        hpm, hpw = hpm_t.numpy(), hpw_t.numpy()
+        hm = torch.empty(n, dtype=torch.int32, pin_memory=True).numpy()
+        ctx.solve(hpm, hpw, out=hm)
+        e2e = []
+        for _ in range(3 if n > 5000 else reps):
+            t0 = time.perf_counter()
+            _, est = ctx.solve(hpm, hpw, out=hm)
+            e2e.append((time.perf_counter() - t0) * 1e3)
+        assert np.array_equal(hm, got), f"{name}: host-input matching differs from the device-input one"
+        rec = {"n": n, "kind": kind, "seed": seed, "param": param, "mode": best["mode"],
+               "proposals": best["proposals"], "device_ms": round(best["total_ms"], 4),
+               "device_ms_runs": [round(x["total_ms"], 4) for x in dev],
+               "phases_ms": {k: round(best[k], 4) for k in ("precheck_ms", "invert_ms", "init_ms", "bulk_ms", "tail_ms",
+                                                           "core_ms", "post_ms")},
+               "roofline": config_roofline(n, best, best["total_ms"]),
+               "e2e_ms": round(min(e2e), 3), "e2e_path": "C ABI smp_b200_solve with pinned host buffers"}
+        if have_ref:
+            prob = oracle.RefProblem(hpm, hpw)
+            engines = (0, 3) if n <= 5000 else (3,)
+            for eng in engines:
+                ref_match, ms = prob.solve(eng)
+                assert np.array_equal(ref_match, got), f"{name}: {oracle.REF_ENGINES[eng]} matching differs"
+                rec[oracle.REF_ENGINES[eng]] = {"ms": round(sum(ms), 3), "phases_ms": [round(x, 3) for x in ms],
+                                                "threads": 1 if eng == 0 else oracle.ref_threads()}
+            prob.close()
+        out[name] = rec
+        del hpm_t, hpw_t
+    if have_ref and c2_pm is not None:
+        # the reference's sequential engine on the headline instance: one run
+        prob = oracle.RefProblem(c2_pm, c2_pw)
+        ref_match, ms = prob.solve(0)
+        prob.close()
+        assert np.array_equal(ref_match, c2_match), "Gs-Seq-CPU matching differs from the GPU's"
+        out["n30000_uniform_gs_seq_cpu"] = {"ms": round(sum(ms), 3), "phases_ms": [round(x, 3) for x in ms],
+                                            "threads": 1, "engine": "Gs-Seq-CPU (src/smp/smp_engine_gs_1.cu)"}
+    out["cpu_engines_note"] = ("reference engines compiled from their sources into oracle/_ref; times are their own "
+                               "precheck + init + core stopwatch")
+    return out
 
 
 def cpu_baseline(args, h_pm, h_pw, gpu_match, ctx) -> dict:
@@ -680,23 +830,37 @@ def run_init_study(args) -> None:
     ctx.close()
 
 
-def run_bamboo_study(args) -> None:
+class stdout_to_stderr:
+    """Sends file descriptor 1 to stderr for the duration (native code that
+    prints to stdout included)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def bamboo_cases(ctx, cases) -> list[dict]:
     """The reference's own GPU engine, SmpEngineBamboo (the BambooSMP solve:
     GPU rank and PR matrices, La3F9CoreKernel, a host monitor that finishes a
     last lone chain on the CPU; src/smp/smp_engine_bamboo.cu), built from its
     sources into oracle/_ref/libsmpref_bamboo{,_o3}.so, beside this library's
-    solve on the same B200 and the same instances.  The reference's figures
-    are its engine's own precheck/init/core stopwatch (AbsSmpEngine,
-    smp_engine_abs.h:10-36), with its untimed list upload and PR-matrix
-    download listed apart; ours are the device-input solve (CUDA events) and
-    the host-input solve through the C ABI (wall clock).  Matchings must be
-    identical.  One JSON line per case."""
+    solve on the same B200 and the same instances (kind, n, seed).  The
+    reference's figures are its engine's own precheck/init/core stopwatch
+    (AbsSmpEngine, smp_engine_abs.h:10-36), with its untimed list upload and
+    PR-matrix download listed apart; ours are the device-input solve (CUDA
+    events) and the host-input solve through the C ABI (wall clock).
+    Matchings must be identical.  One record per case."""
     import ctypes
 
     import numpy as np
     import torch
-
-    import pactae_b200 as pb
 
     libs = {}
     for tag, name in (("ptxas_O0_release", "libsmpref_bamboo.so"), ("ptxas_O3", "libsmpref_bamboo_o3.so")):
@@ -707,8 +871,8 @@ def run_bamboo_study(args) -> None:
                                              ctypes.POINTER(ctypes.c_double)]
             libs[tag] = lib
     if not libs:
-        print(json.dumps({"bamboo_study": "unavailable", "why": "oracle/_ref/libsmpref_bamboo*.so not built"}))
-        return
+        return [{"bamboo_study": "unavailable", "why": "oracle/_ref/libsmpref_bamboo*.so not built"}]
+
     def mem_available() -> int:
         with open("/proc/meminfo") as f:
             for line in f:
@@ -716,16 +880,14 @@ def run_bamboo_study(args) -> None:
                     return int(line.split()[1]) * 1024
         return 0
 
-    ctx = pb.Context(0)
-    for case in args.bamboo_cases.split(","):
-        kind, n, seed = (int(x) for x in case.split(":"))
+    records = []
+    for kind, n, seed in cases:
         # host bytes at peak: our pinned lists (8 n^2), the engine's SmpObj and
         # its construction copies (16 n^2) and its host PR matrix (8 n^2)
         need = 32 * n * n
         if mem_available() < 2 * need:
-            print(json.dumps({"bamboo_study": f"kind {kind} n={n} seed {seed}", "unavailable":
-                              f"host memory: {mem_available() >> 30} GiB available, {2 * need >> 30} GiB wanted"}),
-                  flush=True)
+            records.append({"bamboo_study": f"kind {kind} n={n} seed {seed}", "unavailable":
+                            f"host memory: {mem_available() >> 30} GiB available, {2 * need >> 30} GiB wanted"})
             continue
         dpm, dpw = ctx.generate(kind, n, seed)
         ours_match, _ = ctx.solve(dpm, dpw)  # warm-up
@@ -755,7 +917,8 @@ def run_bamboo_study(args) -> None:
             for _ in range(2):  # the first run warms the engine up
                 ms = (ctypes.c_double * 6)()
                 got = np.empty(n, np.int32)
-                rc = lib.ref_bamboo_solve(hpm.ctypes.data, hpw.ctypes.data, n, got.ctypes.data, ms)
+                with stdout_to_stderr():  # the engine prints its progress; the bench's stdout is its JSON line
+                    rc = lib.ref_bamboo_solve(hpm.ctypes.data, hpw.ctypes.data, n, got.ctypes.data, ms)
                 runs.append((rc, list(ms), got))
             rc, ms, got = runs[-1]
             # engine-reported total: precheck + init + core with the lists
@@ -771,13 +934,24 @@ def run_bamboo_study(args) -> None:
                         "engine_total_ms_first_run": round(sum(runs[0][1][:3]), 3)}
         best_dev = min(r["engine_total_ms"] for r in ref.values())
         best_e2e = min(r["end_to_end_ms"] for r in ref.values())
-        print(json.dumps({"bamboo_study": f"kind {kind} n={n} seed {seed}", "n": n, "kind": kind, "seed": seed,
-                          "reference_smp_engine_bamboo": ref,
-                          "ours": {"device_input_ms": round(min(dev_ms), 3), "host_input_e2e_ms": round(min(e2e_ms), 2)},
-                          "speedup_vs_best_reference": {
-                              "device_input_vs_engine_total": round(best_dev / min(dev_ms), 1),
-                              "host_input_e2e_vs_end_to_end": round(best_e2e / min(e2e_ms), 1)}}), flush=True)
+        records.append({"bamboo_study": f"kind {kind} n={n} seed {seed}", "n": n, "kind": kind, "seed": seed,
+                        "reference_smp_engine_bamboo": ref,
+                        "ours": {"device_input_ms": round(min(dev_ms), 3), "host_input_e2e_ms": round(min(e2e_ms), 2)},
+                        "speedup_vs_best_reference": {
+                            "device_input_vs_engine_total": round(best_dev / min(dev_ms), 1),
+                            "host_input_e2e_vs_end_to_end": round(best_e2e / min(e2e_ms), 1)}})
         del hpm_t, hpw_t
+    return records
+
+
+def run_bamboo_study(args) -> None:
+    """--bamboo-study: bamboo_cases over --bamboo-cases, one JSON line each."""
+    import pactae_b200 as pb
+
+    ctx = pb.Context(0)
+    cases = [tuple(int(x) for x in c.split(":")) for c in args.bamboo_cases.split(",")]
+    for rec in bamboo_cases(ctx, cases):
+        print(json.dumps(rec), flush=True)
     ctx.close()
 
 

@@ -32,6 +32,8 @@ constexpr int kRankTailWindow = 256;
 // whole CTA scanning each).
 constexpr int kCoopChains = 4;
 constexpr int kU16MaxN = 65535;
+// From this n the colour-tagged query inversion runs 384-thread CTAs.
+constexpr int kLongRowN = 16384;
 
 inline bool valid_ctx(const smp_ctx *ctx) { return ctx != nullptr && ctx->c.stream != nullptr; }
 
@@ -246,12 +248,13 @@ int enqueue_query_index(Ctx &c) {
 int enqueue_qinvert(Ctx &c, int w0, int w1) {
   // n <= kColorMaxN: the pipelined kernel with colour-tagged slots;
   // larger n: the one with a clearing pass per row.
-  const auto kernel = c.n <= kColorMaxN ? k_qinvert_c : k_qinvert;
+  const bool long_rows = c.n >= kLongRowN;
+  const auto kernel = c.n > kColorMaxN ? k_qinvert : long_rows ? k_qinvert_c<384> : k_qinvert_c<256>;
   const size_t smem = row_smem_bytes<uint16_t>(c.n);
   if (allow_dynamic_smem(c, kernel) !=
       cudaSuccess)
     return c.fail_cuda("k_qinvert smem attribute");
-  const int block = c.n <= kColorMaxN ? 256 : 512;
+  const int block = c.n > kColorMaxN ? 512 : long_rows ? 384 : 256;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess) {
     cudaGetLastError();

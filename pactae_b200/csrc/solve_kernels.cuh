@@ -533,7 +533,10 @@ __device__ __forceinline__ void scatter_c(uint16_t *srow, int m, int r, uint32_t
   }
 }
 
-__global__ void __launch_bounds__(256) k_qinvert_c(const int32_t *__restrict__ pref_w, int n, int K, int qcap,
+// kThreads: 384 for long rows (n = 30000: 0.865 ms against 0.922 with 256),
+// 256 for shorter ones (n = 12000: 0.198 ms against 0.204 with 384).
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads) k_qinvert_c(const int32_t *__restrict__ pref_w, int n, int K, int qcap,
                                                       const int32_t *__restrict__ qcnt,
                                                       const uint32_t *__restrict__ qlist,
                                                       uint32_t *__restrict__ prefix, Control *ctrl, int w0, int w1) {
