@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(256) k_swap_screen(const int32_t *__restrict__
         if (tid < s.head) differs |= __ldcs(s.row + tid) != __ldg(pref_w + tid);
         const int c0 = s.head + 4 * s.nq;
         if (tid < s.tail) differs |= __ldcs(s.row + c0 + tid) != __ldg(pref_w + c0 + tid);
-        if (differs) atomicExch(&ctrl->w_differ, 1);
+        if (__syncthreads_or(differs) && tid == 0) atomicExch(&ctrl->w_differ, 1);  // one flag per CTA and row
       }
       const auto mark = [&](int v) {
         if (static_cast<unsigned>(v) >= static_cast<unsigned>(n)) {

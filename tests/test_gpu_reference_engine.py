@@ -58,3 +58,23 @@ def test_matches_smp_engine_bamboo(ctx, bamboo, kind, n, param):
     ours, _ = ctx.solve(pm, pw)
     assert np.array_equal(ours, ref)
     assert np.array_equal(ref, oracle.gs_seq(pm, pw)[0])
+
+
+INIT_GPU = ROOT / "oracle" / "_ref" / "libsmpref_gpu.so"
+
+
+@pytest.mark.skipif(not INIT_GPU.exists(), reason="oracle/_ref/libsmpref_gpu.so not built")
+@pytest.mark.parametrize("kind,n", [(pb.SMP_GEN_REF_CONGESTED, 1000), (pb.SMP_GEN_UNIFORM, 2999),
+                                    (pb.SMP_GEN_REF_CONGESTED, 5000)])
+def test_invert_matches_smp_init_gpu(ctx, kind, n):
+    # The reference's GPU init engine SmpInitEngine3 ("Smp-Init-Gpu",
+    # include/smp/smp_init_3.h:68-95, the engine its init study times) and
+    # smp_b200_invert must produce the same int32 rank matrix.
+    lib = ctypes.CDLL(str(INIT_GPU))
+    lib.ref_gpu_rank.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
+    pm, pw = oracle.generate(kind, n, 2)
+    pm = np.ascontiguousarray(pm, np.int32)
+    pw = np.ascontiguousarray(pw, np.int32)
+    want = np.empty((n, n), np.int32)
+    assert lib.ref_gpu_rank(pm.ctypes.data, pw.ctypes.data, n, want.ctypes.data) == 0
+    assert np.array_equal(ctx.invert(pw), want)
