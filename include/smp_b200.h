@@ -343,10 +343,10 @@ SMP_B200_API void smp_b200_server_destroy(smp_server *srv);
  * All scratch lives in one file-scope device array of 2 MiB + 256 bytes that
  * every GPU loading the library keeps until exit, so n is limited to
  * SMP_B200_STATIC_MAX_N (larger n returns SMP_ERR_UNSUPPORTED before
- * anything runs).  The first call on a device looks up the array's device
- * address, so make it before any stream capture.  Every call shares the
- * array: calls that overlap on the GPU race, so order them on one stream.
- * Returns after the work has finished. */
+ * anything runs).  The call is synchronous: it waits on the stream for the
+ * result header, so it cannot be made on a stream under capture (that would
+ * invalidate the capture) or captured into a graph.  Every call shares the
+ * array: calls that overlap on the GPU race, so order them on one stream. */
 SMP_B200_API int smp_b200_solve_static(const int32_t *pref_m, const int32_t *pref_w, int32_t n,
                                        int32_t *match_out, int64_t *proposals, void *stream);
 

@@ -95,11 +95,13 @@ struct DeviceGuard {
   }
 };
 
-// A fixed set of host threads that run one job at a time: run(f) calls
-// f(i, count) on every worker i and returns when all have finished.  Started
-// once per context, so a call costs a wake-up, not a thread creation.
 // Entries [begin, end) of src packed to uint16 in dst (host_pack.cpp).
 void pack_u16(const int32_t *src, uint16_t *dst, size_t begin, size_t end, int n);
+
+// A fixed set of host threads that run one job at a time: run(f) calls
+// f(i, count) on every worker i and returns when all have finished; start(f)
+// returns at once and wait() when the job has finished.  Started once per
+// context, so a job costs a wake-up, not a thread creation.
 
 class HostPool {
  public:
@@ -116,11 +118,20 @@ class HostPool {
   }
   int size() const { return static_cast<int>(threads_.size()); }
   void run(const std::function<void(int, int)> &f) {
+    start(f);
+    wait();
+  }
+  void start(std::function<void(int, int)> f) {
     std::unique_lock<std::mutex> lock(mu_);
-    job_ = &f;
+    done_.wait(lock, [this] { return pending_ == 0; });
+    owned_ = std::move(f);
+    job_ = &owned_;
     pending_ = size();
     ++generation_;
     cv_.notify_all();
+  }
+  void wait() {
+    std::unique_lock<std::mutex> lock(mu_);
     done_.wait(lock, [this] { return pending_ == 0; });
     job_ = nullptr;
   }
@@ -145,10 +156,70 @@ class HostPool {
   std::vector<std::thread> threads_;
   std::mutex mu_;
   std::condition_variable cv_, done_;
+  std::function<void(int, int)> owned_;
   const std::function<void(int, int)> *job_ = nullptr;
   unsigned generation_ = 0;
   int pending_ = 0;
   bool stop_ = false;
+};
+
+// Sends int32 host matrices to device memory packed to uint16, half the
+// bytes on the host link.  Each of the pool's workers owns a CUDA stream and
+// two pinned slots of kSlotEntries entries: it packs a piece of a matrix
+// into one slot with ordinary stores -- the slot stays in the host's cache,
+// where the copy engine reads it back, so the only host DRAM traffic is the
+// read of the source -- and queues the slot's copy on its stream while it
+// packs the next piece into the other.  Pieces are dealt to the workers in
+// turn.  Each matrix is cut into row groups; when a worker has queued its
+// pieces of a group it records the group's event on its stream, and
+// wait_group makes a stream wait for every worker's event of that group, so
+// device work on a group starts as soon as its rows have landed.
+class HostLink {
+ public:
+  static constexpr size_t kSlotEntries = size_t{1} << 20;  // 2 MiB of uint16
+  static constexpr int kMaxGroups = 32;
+  struct Part {
+    const int32_t *src;  // host, rows x n
+    uint16_t *dst;       // device, rows x n
+    int rows;
+  };
+  HostLink() = default;
+  HostLink(const HostLink &) = delete;
+  HostLink &operator=(const HostLink &) = delete;
+  ~HostLink();
+  // Streams, events and pinned slots for the pool's workers.  SMP_OK, or
+  // SMP_ERR_OOM / SMP_ERR_CUDA (the link is then unusable).
+  int open(HostPool *pool);
+  // Packs and sends parts[0..nparts) (at most two), each cut into `groups`
+  // row groups; group g of part p is global group p * groups + g.  The
+  // copies are queued after the work already queued on `after`.
+  int start(const Part *parts, int nparts, int n, int groups, cudaStream_t after);
+  // Rows [r0, r1) of global group g (row0 of that group's part).
+  void group_rows(int g, int *part, int *r0, int *r1) const;
+  // Blocks until every worker has queued its pieces of global group g, then
+  // makes `stream` wait for them on the device.
+  int wait_group(int g, cudaStream_t stream);
+  // Waits for the workers and their copies; SMP_ERR_CUDA if a call failed.
+  int finish();
+  const std::string &error() const { return error_; }
+
+ private:
+  void work(int t);
+  HostPool *pool_ = nullptr;
+  int workers_ = 0;
+  std::vector<cudaStream_t> streams_;
+  std::vector<cudaEvent_t> slot_ev_;   // 2 per worker
+  std::vector<cudaEvent_t> group_ev_;  // kMaxGroups per worker
+  std::vector<uint16_t *> slots_;      // 2 per worker, pinned
+  cudaEvent_t ready_ = nullptr;
+  Part parts_[2] = {};
+  int nparts_ = 0, n_ = 0, groups_ = 0;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  int queued_[kMaxGroups] = {};
+  bool failed_ = false;
+  bool running_ = false;
+  std::string error_;
 };
 
 struct Control;  // common.cuh
@@ -189,14 +260,12 @@ struct Ctx {
   int known_mode = -1;
 
   DeviceBuf d_pref_m, d_pref_w, d_rank, d_rankT, d_pr, d_prefix, d_bid, d_tailq, d_seen, d_ctrl, d_match;
-  DeviceBuf d_pw16;  // pref_w packed to uint16 (host-input solves)
+  DeviceBuf d_pw16, d_pm16;  // pref_w and pref_m packed to uint16 (host-input solves)
   DeviceBuf d_swap_pos;  // women-proposing solves: position of each woman in the men's shared list
-  // Host-input solves: a ring of pinned buffers the chunks of pref_w are
-  // packed into while earlier ones are copied, and the threads that pack.
-  static constexpr int kStageDepth = 3;
-  uint16_t *h_stage[kStageDepth] = {};
-  size_t h_stage_elems = 0;
+  // Host-input solves: the host threads that pack and screen, and the link
+  // that sends packed rows through them (created on first use).
   std::unique_ptr<HostPool> pack_pool;
+  std::unique_ptr<HostLink> link;
   DeviceBuf d_husband, d_prank;
   DeviceBuf d_qcnt, d_qlist;
   DeviceBuf gen_keys_a, gen_keys_b, gen_seg, gen_temp, gen_aux;
@@ -207,8 +276,8 @@ struct Ctx {
   static constexpr int kCopyChunks = 16;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_chunk[kCopyChunks] = {};
-  std::array<DeviceBuf *, 22> buffers() {
-    return {&d_pref_m, &d_pref_w, &d_pw16, &d_rank,    &d_rankT,    &d_pr,     &d_prefix, &d_bid,    &d_tailq,
+  std::array<DeviceBuf *, 23> buffers() {
+    return {&d_pref_m, &d_pref_w, &d_pw16, &d_pm16, &d_rank,    &d_rankT,    &d_pr,     &d_prefix, &d_bid,    &d_tailq,
             &d_seen,   &d_ctrl,   &d_match,   &d_husband,  &d_prank,  &d_qcnt,   &d_qlist,
             &gen_keys_a, &gen_keys_b, &gen_seg, &gen_temp, &gen_aux, &d_swap_pos};
   }

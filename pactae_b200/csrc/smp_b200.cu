@@ -26,6 +26,8 @@ constexpr int kDefaultTailWindow = 256;
 // Query buckets hold up to 1.5 K + 32 pairs per woman (at most n).
 int query_capacity(int n, int K) { return std::min(n, K + K / 2 + 32); }
 // Host-pointer solves of at least this n stream their inputs (solve_streamed).
+// Rank-mode host-input solves send each list in this many row groups.
+constexpr int kRankGroups = 8;
 constexpr int kStreamMinN = 4096;
 constexpr int kRankTailWindow = 256;
 // Chains left when k_tail hands the rest to k_tail_coop (one at a time, the
@@ -839,57 +841,83 @@ int solve_finish(Ctx &c, uint32_t flags, smp_stats *st) {
 // the work.  A query-mode solve reads only each man's first K choices of
 // pref_m (plus his first choice for the precheck), and pref_w row by row in
 // the inversion.  So: copy the first K columns of pref_m, run the precheck
-// and read its decision; in query mode stream pref_w in row chunks on a
-// second stream and invert each chunk as it lands, and copy the rest of
-// pref_m only if a man goes beyond his prefix (the rank-mode retry).  A
-// rank-mode or perfect instance falls back to copying what it needs first.
-// Two host round trips (after the precheck and after round 0) are the price.
+// and read its decision; in query mode send pref_w packed to uint16 in row
+// groups and invert each group as it lands, and copy the rest of pref_m only
+// if a man goes beyond his prefix (the rank-mode retry).  A rank-mode
+// instance sends both lists packed and widens them on the device, unless
+// the men may share one list: then pref_w crosses as it is while the host
+// threads compare the men's rows, and only row 0 of pref_m follows if they
+// are all alike.  A perfect instance copies nothing more.  Two host round
+// trips (after the precheck and after round 0) are the price.
 bool streamed_fits(const Ctx &c, uint32_t flags) {
   return !(flags & (SMP_F_DEVICE_PTRS | SMP_F_VALIDATE | SMP_F_CHECK)) && c.query_ok && c.K > 0 && c.K < c.n &&
          c.tail_threshold > 0 && c.n >= kStreamMinN;
 }
 
-// Host-input query solves stream pref_w packed to uint16 -- half the bytes
-// on the host link, which is what an n = 30000 host-input solve waits for --
-// when the colour-tagged inversion applies (n <= kColorMaxN) and the host
-// has threads to pack with.  Sets up the pinned staging ring and the packing
-// threads on first use; false if packing does not apply.
-bool pack_ready(Ctx &c) {
+// Host-input solves send their lists packed to uint16 -- half the bytes on
+// the host link, which is what a host-input solve of n = 30000 waits for --
+// through the context's HostLink, when the host has threads to pack with.
+// Sets up the packed device buffers (pref_w's, and pref_m's when both lists
+// cross), the host threads and the link on first use; false if packing does
+// not apply (the caller then copies int32 rows).
+bool link_ready(Ctx &c, bool both) {
   const int n = c.n;
-  if (n > kColorMaxN || n < 8) return false;
+  if (n > 65535 || n < 8) return false;
   const unsigned hw = std::thread::hardware_concurrency();
   if (hw < 4) return false;
-  const size_t chunk = static_cast<size_t>((n + Ctx::kCopyChunks - 1) / Ctx::kCopyChunks + 1) * n;
-  if (c.h_stage_elems < chunk) {
-    for (auto &h : c.h_stage) {
-      if (h) cudaFreeHost(h);
-      h = nullptr;
-    }
-    c.h_stage_elems = 0;
-    for (auto &h : c.h_stage) {
-      if (cudaMallocHost(reinterpret_cast<void **>(&h), sizeof(uint16_t) * chunk) != cudaSuccess) {
-        cudaGetLastError();
-        for (auto &g : c.h_stage) {
-          if (g) cudaFreeHost(g);
-          g = nullptr;
-        }
-        return false;
-      }
-    }
-    c.h_stage_elems = chunk;
-  }
-  if (c.d_pw16.ensure(sizeof(uint16_t) * static_cast<size_t>(n) * n)) return false;
-  // twelve packing threads: on a 16-core host with the copy engine reading
-  // the staging at the same time, eight were slower and sixteen no faster
+  const size_t bytes = sizeof(uint16_t) * static_cast<size_t>(n) * n;
+  if (c.d_pw16.ensure(bytes)) return false;
+  if (both && c.d_pm16.ensure(bytes)) return false;
+  // twelve threads: on a 16-core host, 8, 12 and 16 packed and sent an
+  // n = 30000 list in the same 37 ms, bound by reading it from host DRAM
   if (!c.pack_pool) c.pack_pool.reset(new (std::nothrow) HostPool(static_cast<int>(std::min(hw, 12u))));
-  return c.pack_pool != nullptr;
+  if (!c.pack_pool) return false;
+  if (!c.link) {
+    c.link.reset(new (std::nothrow) HostLink());
+    if (!c.link || c.link->open(c.pack_pool.get()) != SMP_OK) {
+      c.link.reset();
+      return false;
+    }
+  }
+  return true;
 }
 
-// count entries of src into uint16 dst on the packing threads; an entry
-// outside [0, n) becomes a value >= n, which the inversion reports.
-void pack_rows(Ctx &c, const int32_t *src, uint16_t *dst, size_t count, int n) {
-  const auto job = [&](int i, int parts) { pack_u16(src, dst, count * i / parts, count * (i + 1) / parts, n); };
-  c.pack_pool->run(job);
+int enqueue_widen16(Ctx &c, const uint16_t *src, int32_t *dst, size_t begin, size_t end) {
+  if (begin >= end) return SMP_OK;
+  const size_t steps = (end - (begin & ~size_t{7}) + 7) / 8;
+  const int grid = static_cast<int>(std::min<size_t>(static_cast<size_t>(c.sm_count) * 8, (steps + 255) / 256));
+  k_widen16<<<grid, 256, 0, c.stream>>>(src, dst, begin, end);
+  c.launches++;
+  return c.check_launch("k_widen16");
+}
+
+// Sends parts through the link in `groups` row groups per part and, as each
+// group lands, enqueues on c.stream what uses its rows (on_group(part, r0,
+// r1)).  Returns after every copy has finished.
+template <typename OnGroup>
+int send_packed(Ctx &c, const HostLink::Part *parts, int nparts, int groups, OnGroup on_group) {
+  HostLink &link = *c.link;
+  int rc = link.start(parts, nparts, c.n, groups, c.stream);
+  if (rc) {
+    c.last_error = link.error();
+    return rc;
+  }
+  for (int g = 0; !rc && g < nparts * groups; ++g) {
+    int p = 0, r0 = 0, r1 = 0;
+    link.group_rows(g, &p, &r0, &r1);
+    rc = link.wait_group(g, c.stream);
+    if (rc)
+      c.last_error = link.error();
+    else if (r0 < r1)
+      rc = on_group(p, r0, r1);
+  }
+  // the workers read the caller's buffers: join them even after an error
+  const int lr = link.finish();
+  if (!rc && lr) {
+    rc = lr;
+    c.last_error = link.error();
+  }
+  return rc;
 }
 
 // Does every row of the host matrix pref_m equal row 0?  Rows are compared
@@ -961,15 +989,25 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
                             c.mode_cfg == 0 && swap_screen_smem(n) <= c.smem_optin;
     bool shared = false;
     if (!c.h_ctrl->perfect) {
-      if (cudaMemcpyAsync(dw, pref_w, row * n, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
-        rc = c.fail_cuda("pref_w copy");
-      if (!rc && try_shared) {
-        if (cudaMemcpyAsync(dm + c.K, pref_m + c.K, sizeof(int32_t) * (n - c.K), cudaMemcpyHostToDevice, c.stream) !=
-            cudaSuccess)
-          rc = c.fail_cuda("pref_m row 0 copy");
-        if (!rc) shared = host_rows_equal_row0(c, pref_m, n);
+      if (!try_shared && link_ready(c, true)) {
+        // Both lists cross packed, pref_w first; each row group is widened
+        // back to int32 on the device as it lands.
+        const HostLink::Part parts[2] = {{pref_w, c.d_pw16.as<uint16_t>(), n}, {pref_m, c.d_pm16.as<uint16_t>(), n}};
+        rc = send_packed(c, parts, 2, kRankGroups, [&](int p, int r0, int r1) {
+          return enqueue_widen16(c, p ? c.d_pm16.as<uint16_t>() : c.d_pw16.as<uint16_t>(), p ? dm : dw,
+                                 static_cast<size_t>(r0) * n, static_cast<size_t>(r1) * n);
+        });
+      } else {
+        if (cudaMemcpyAsync(dw, pref_w, row * n, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+          rc = c.fail_cuda("pref_w copy");
+        if (!rc && try_shared) {
+          if (cudaMemcpyAsync(dm + c.K, pref_m + c.K, sizeof(int32_t) * (n - c.K), cudaMemcpyHostToDevice,
+                              c.stream) != cudaSuccess)
+            rc = c.fail_cuda("pref_m row 0 copy");
+          if (!rc) shared = host_rows_equal_row0(c, pref_m, n);
+        }
+        if (!rc && !shared) rc = copy_rest_of_m();
       }
-      if (!rc && !shared) rc = copy_rest_of_m();
     }
     if (!rc && cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
     if (!rc && shared) rc = solve_swapped(c, flags, match_out, swapped, true);
@@ -980,41 +1018,27 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
     if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
     rc = init_buffers(c);
     if (!rc) rc = enqueue_query_index(c);
-    const bool packed = !rc && pack_ready(c);
-    // Packed chunks go through the staging ring; chunks 4 and 12 of 16 cross
-    // as int32 straight from the caller's buffer, keeping the link busy
-    // while the packing threads -- the slower side -- work.
-    int ring[Ctx::kStageDepth] = {};
-    int staged = 0;
-    for (int k = 0; !rc && k < Ctx::kCopyChunks; ++k) {
+    const bool packed = !rc && n <= kColorMaxN && link_ready(c, false);
+    if (packed) {
+      // pref_w crosses packed in row groups; each group's inversion waits
+      // only for its own rows
+      const HostLink::Part part = {pref_w, c.d_pw16.as<uint16_t>(), n};
+      rc = send_packed(c, &part, 1, Ctx::kCopyChunks,
+                       [&](int, int r0, int r1) { return enqueue_qinvert16(c, r0, r1); });
+    }
+    for (int k = 0; !rc && !packed && k < Ctx::kCopyChunks; ++k) {
       const int r0 = static_cast<int>(static_cast<int64_t>(n) * k / Ctx::kCopyChunks);
       const int r1 = static_cast<int>(static_cast<int64_t>(n) * (k + 1) / Ctx::kCopyChunks);
       if (r0 == r1) continue;
       const size_t off = static_cast<size_t>(r0) * n;
-      const bool pack = packed && k % 8 != 4;
-      cudaError_t e;
-      if (pack) {
-        // wait for the copy of the chunk that last used this staging buffer
-        const int slot = staged % Ctx::kStageDepth;
-        uint16_t *stage = c.h_stage[slot];
-        if (staged >= Ctx::kStageDepth && cudaEventSynchronize(c.ev_chunk[ring[slot]]) != cudaSuccess) {
-          rc = c.fail_cuda("staging wait");
-          break;
-        }
-        ring[slot] = k;
-        ++staged;
-        pack_rows(c, pref_w + off, stage, static_cast<size_t>(r1 - r0) * n, n);
-        e = cudaMemcpyAsync(c.d_pw16.as<uint16_t>() + off, stage, sizeof(uint16_t) * static_cast<size_t>(r1 - r0) * n,
-                            cudaMemcpyHostToDevice, c.copy_stream);
-      } else {
-        e = cudaMemcpyAsync(dw + off, pref_w + off, row * (r1 - r0), cudaMemcpyHostToDevice, c.copy_stream);
-      }
-      if (e != cudaSuccess || cudaEventRecord(c.ev_chunk[k], c.copy_stream) != cudaSuccess ||
+      if (cudaMemcpyAsync(dw + off, pref_w + off, row * (r1 - r0), cudaMemcpyHostToDevice, c.copy_stream) !=
+              cudaSuccess ||
+          cudaEventRecord(c.ev_chunk[k], c.copy_stream) != cudaSuccess ||
           cudaStreamWaitEvent(c.stream, c.ev_chunk[k], 0) != cudaSuccess) {
         rc = c.fail_cuda("pref_w chunk copy");
         break;
       }
-      rc = pack ? enqueue_qinvert16(c, r0, r1) : enqueue_qinvert(c, r0, r1);
+      rc = enqueue_qinvert(c, r0, r1);
     }
     if (!rc && cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
     if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
@@ -1025,9 +1049,9 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
     if (!rc && c.h_ctrl->retry && !c.h_ctrl->status) {
       c.known_mode = -1;
       rc = copy_rest_of_m();
-      // the rank-mode retry inverts pref_w itself: the packed chunks will not do
-      if (!rc && packed && cudaMemcpyAsync(dw, pref_w, row * n, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
-        rc = c.fail_cuda("pref_w copy");
+      // the rank-mode retry inverts int32 rows: widen the packed ones
+      if (!rc && packed)
+        rc = enqueue_widen16(c, c.d_pw16.as<uint16_t>(), dw, 0, static_cast<size_t>(n) * n);
       if (!rc) rc = enqueue_retry_round<uint16_t>(c);
     }
   }
@@ -1146,8 +1170,7 @@ void smp_b200_destroy(smp_ctx *ctx) {
       if (e) cudaEventDestroy(e);
     if (c.copy_stream) cudaStreamDestroy(c.copy_stream);
     if (c.h_ctrl) cudaFreeHost(c.h_ctrl);
-    for (auto &h : c.h_stage)
-      if (h) cudaFreeHost(h);
+    c.link.reset();
     c.pack_pool.reset();
     if (c.stream) cudaStreamDestroy(c.stream);
   }

@@ -802,6 +802,33 @@ __global__ void __launch_bounds__(256) k_qinvert_p16(const uint16_t *__restrict_
   if (bad) report(ctrl, kStatusInvalidInput, -1);
 }
 
+// Entries [begin, end) of a matrix packed to uint16 on the host, widened
+// back to the int32 rows that rank-mode solves read.  A packed 0xFFFF -- what
+// the packing makes of an entry outside [0, n) -- widens to 65535, still
+// >= n (n <= 65535 here), so the kernels that read the entry report it.
+// Eight entries per thread step: one 16-byte load and two 16-byte stores
+// where all eight lie inside the span, one by one at its ragged ends.
+__global__ void __launch_bounds__(256) k_widen16(const uint16_t *__restrict__ src, int32_t *__restrict__ dst,
+                                                 size_t begin, size_t end) {
+  const size_t base = begin & ~size_t{7};
+  const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x * 8;
+  for (size_t i = base + (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 8; i < end; i += stride) {
+    if (i >= begin && i + 8 <= end) {
+      const uint4 v = __ldcs(reinterpret_cast<const uint4 *>(src + i));
+      const int4 lo = make_int4(static_cast<int>(v.x & 0xFFFFu), static_cast<int>(v.x >> 16),
+                                static_cast<int>(v.y & 0xFFFFu), static_cast<int>(v.y >> 16));
+      const int4 hi = make_int4(static_cast<int>(v.z & 0xFFFFu), static_cast<int>(v.z >> 16),
+                                static_cast<int>(v.w & 0xFFFFu), static_cast<int>(v.w >> 16));
+      int4 *out = reinterpret_cast<int4 *>(dst + i);
+      out[0] = lo;
+      out[1] = hi;
+    } else {
+      const size_t j1 = i + 8 < end ? i + 8 : end;
+      for (size_t j = i < begin ? begin : i; j < j1; ++j) dst[j] = src[j];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Bulk proposals on every SM.  Each warp carries one free man at a time
 // (man_step above, 64-bit bids in HBM).  A man accepted by a free woman

@@ -17,8 +17,10 @@
 //   - n <= SMP_B200_STATIC_MAX_N (1024); larger n is rejected with
 //     SMP_ERR_UNSUPPORTED before anything runs.
 //   - The first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (with that device current) and caches it; make
-//     that first call before any stream capture begins.
+//     cudaGetSymbolAddress (with that device current) and caches it.
+//   - Every call is synchronous: it copies the result header back to the
+//     host and waits on the stream, so no call can run on a stream under
+//     capture.
 //   - All calls share the one array, which keeps the last call's contents.
 //     Each call overwrites the rank matrix and clears the header itself, but
 //     calls whose work overlaps on the GPU (different streams, different host

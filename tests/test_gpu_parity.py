@@ -486,3 +486,54 @@ def test_host_input_men_sharing_one_list(case):
     want, props = oracle.gs_seq(pm, pw)
     assert np.array_equal(match, want) and st["proposals"] == props
     assert st["mode"] == (0 if case == "twisted" else 3)
+
+
+@pytest.mark.parametrize("defect", ["none", "duplicate", "negative", "wraps_to_valid", "men_wrap"])
+def test_host_input_rank_mode_sends_packed_lists(defect):
+    # Rank-mode host-input solves send both lists packed to 16 bits, in row
+    # groups, and widen each group back to int32 on the device.  A defect must
+    # survive packing: a duplicate stays one, and -1 or v + 65536 pack to
+    # 0xFFFF, which widens to 65535 >= n.  The defect sits in the last row
+    # group of pref_w; "men_wrap" puts v + 65536 in every man's second choice,
+    # which correlated lists make many men reach.
+    n = 4099
+    pm, pw = oracle.generate(pb.SMP_GEN_CORRELATED, n, 29, 0, 500)
+    pm, pw = pm.copy(), pw.copy()
+    row = n - 3
+    if defect == "duplicate":
+        pw[row, 5] = pw[row, 6]
+    elif defect == "negative":
+        pw[row, int(np.nonzero(pw[row] == 0)[0][0])] = -1
+    elif defect == "wraps_to_valid":
+        pw[row, 7] += 65536
+    elif defect == "men_wrap":
+        pm[:, 1] += 65536
+    with pb.Context() as c:
+        if defect != "none":
+            with pytest.raises(pb.SmpError) as e:
+                c.solve(pm, pw)
+            assert e.value.status == pb.SMP_ERR_INVALID_INPUT
+            pm, pw = oracle.generate(pb.SMP_GEN_CORRELATED, n, 29, 0, 500)
+        match, st = c.solve(pm, pw)  # the context is still usable
+    want, props = oracle.gs_seq(pm, pw)
+    assert np.array_equal(match, want) and st["proposals"] == props and st["mode"] == 0
+
+
+@pytest.mark.slow
+def test_host_input_rank_mode_above_the_query_limit():
+    # n = 33000, above the query path's 32767: a rank-mode host-input solve
+    # still sends both lists packed (16 bits hold any n <= 65535).  Checked
+    # against the device-input solve of the same lists.
+    import torch
+
+    n = 33000
+    with pb.Context() as c:
+        pm, pw = c.generate(pb.SMP_GEN_CORRELATED, n, seed=5, param=500)
+        want, st0 = c.solve(pm, pw)
+        want = to_host(want)
+        hpm, hpw = to_host(pm), to_host(pw)
+        del pm, pw
+        torch.cuda.empty_cache()
+        got, st = c.solve(hpm, hpw)
+    assert st0["mode"] == 0 and st["mode"] == 0
+    assert np.array_equal(got, want) and st["proposals"] == st0["proposals"]
