@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     ap.add_argument("--batch-count", type=int, default=8192)
     ap.add_argument("--no-plain", action="store_true", help="skip the one-launch-per-instance baseline")
+    ap.add_argument("--no-routing", action="store_true",
+                    help="skip timing the batch with its largest instances routed to the all-SM pipeline")
     ap.add_argument("--serving-loads", default="0.1,0.2,0.3,0.4,0.5,0.6,0.7,0.8,0.9,1.0",
                     help="offered loads as fractions of the measured saturation")
     ap.add_argument("--no-configs", action="store_true",
@@ -503,6 +505,28 @@ def run_batched(ctx, args, dist: Dist) -> dict:
             want, wp = oracle.gs_seq(pm.view(n, n).cpu().numpy(), pw.view(n, n).cpu().numpy())
             assert np.array_equal(mt.cpu().numpy(), want) and props[b] == wp, f"batched instance {b} differs"
         out["oracle_checked"] = len(sample)
+        out["threshold_n"] = out["shape"]["threshold_n"]
+        if not args.no_routing:
+            # The autotuner's routing choice, measured: the tuned shape with
+            # none, or the largest 8, 32 and 128 instances, sent to the
+            # all-SM single-instance pipeline on side streams beside the
+            # persistent kernel (best of 3 graph replays each).
+            shape = out["shape"]
+            cands = []
+            for r in (0, 8, 32, 128):
+                thr = -1 if r == 0 else max(metas[order[r]][0], 1024)
+                routed = sum(1 for n, _ in metas if thr > 0 and n > thr)
+                if r and (routed == 0 or any(c["threshold_n"] == thr for c in cands)):
+                    continue
+                with pb.Batch(ctx, insts, block_threads=shape["block_threads"], ctas_per_sm=shape["ctas_per_sm"],
+                              window=shape["window"], rank_smem_kb=shape["rank_smem_kb"], threshold_n=thr) as b2:
+                    b2.run()
+                    rr = [b2.run() for _ in range(3)]
+                assert all(x == 0 for run in rr for x in run[0]), "a routed batch instance failed"
+                cands.append({"routed": routed, "threshold_n": thr, "ms": round(min(run[2]["ms"] for run in rr), 3)})
+            out["routing"] = {"chosen_threshold_n": out["threshold_n"], "candidates": cands,
+                              "note": "instances above threshold_n run the all-SM single-instance pipeline on "
+                                      "four side streams, forked and joined inside the batch's CUDA graph"}
         if not args.no_plain:
             _, pprops, pst = batch.run_plain()
             assert pst["proposals"] == runs[-1]["proposals"] and pst["failed"] == 0

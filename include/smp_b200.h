@@ -213,7 +213,12 @@ typedef struct smp_batch_cfg {
   int32_t tune;            /* 0 = the autotuner picks every auto field on a  */
                            /* sample of the batch (cached per device, n and  */
                            /* batch size); -1 = fixed defaults               */
-  int32_t reserved[2];
+  int32_t threshold_n;     /* instances with n above it run the all-SM       */
+                           /* single-instance pipeline, on side streams     */
+                           /* beside the persistent kernel; 0 = auto (the    */
+                           /* autotuner times none and the largest 8, 32 and */
+                           /* 128; with tune = -1: none), -1 = none          */
+  int32_t reserved;
 } smp_batch_cfg;
 
 typedef struct smp_batch_stats {
@@ -239,8 +244,9 @@ SMP_B200_API int smp_b200_batch_run(smp_batch *batch, smp_instance *results, smp
 SMP_B200_API int smp_b200_batch_run_plain(smp_batch *batch, smp_instance *results, smp_batch_stats *st);
 SMP_B200_API void smp_b200_batch_destroy(smp_batch *batch);
 /* The shape a batch runs with (after tuning): block_threads, ctas_per_sm,
- * window, use_graph, rank_smem_kb (-1: none) and tune (1: chosen by the
- * autotuner, -1: fixed). */
+ * window, use_graph, rank_smem_kb (-1: none), tune (1: chosen by the
+ * autotuner, -1: fixed) and threshold_n (-1: no instance is routed to the
+ * all-SM pipeline). */
 SMP_B200_API int smp_b200_batch_config(const smp_batch *batch, smp_batch_cfg *out);
 /* create + run + destroy; the status and proposals of inst[] are filled in. */
 SMP_B200_API int smp_b200_solve_batch(smp_ctx *ctx, smp_instance *inst, int32_t count, const smp_batch_cfg *cfg,

@@ -311,7 +311,7 @@ class Batch:
     alive while the batch is used."""
 
     def __init__(self, ctx: Context, instances, block_threads: int = 0, ctas_per_sm: int = 0, window: int = 0,
-                 use_graph: bool = True, rank_smem_kb: int = 0, tune: bool = True):
+                 use_graph: bool = True, rank_smem_kb: int = 0, tune: bool = True, threshold_n: int = 0):
         self.ctx = ctx
         self._keep = list(instances)
         count = len(self._keep)
@@ -332,6 +332,7 @@ class Batch:
         cfg.use_graph = 1 if use_graph else -1
         cfg.rank_smem_kb = rank_smem_kb
         cfg.tune = 0 if tune else -1
+        cfg.threshold_n = threshold_n
         handle = ctypes.c_void_p()
         import torch
 
@@ -348,7 +349,8 @@ class Batch:
         return [r.status for r in results], [r.proposals for r in results], st.as_dict()
 
     def config(self) -> dict:
-        """The shape the batch runs with (after tuning)."""
+        """The shape the batch runs with (after tuning), with threshold_n:
+        instances above it run the all-SM pipeline (-1: none)."""
         cfg = smp_batch_cfg()
         _check(lib.smp_b200_batch_config(self._h, ctypes.byref(cfg)), "smp_b200_batch_config")
         return cfg.as_dict()

@@ -137,7 +137,8 @@ class smp_batch_cfg(ctypes.Structure):
         ("use_graph", ctypes.c_int32),
         ("rank_smem_kb", ctypes.c_int32),
         ("tune", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 2),
+        ("threshold_n", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
     def as_dict(self) -> dict:

@@ -35,15 +35,31 @@ struct smp_batch {
   size_t smem = 0;
   DeviceBuf d_table, d_order, d_queue, d_slabs;
   std::vector<int32_t> order;
+  std::vector<smp_instance> inst;   // the table as given (pointers, n)
   smp_instance *h_table = nullptr;  // pinned copy for results
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Instances with n above threshold_n -- the first `routed` of order[] --
+  // run the single-instance pipeline on the lanes, contexts with their own
+  // streams, forked from the batch's stream while the persistent kernel
+  // takes the rest, and joined before the table is read back.
+  int threshold_n = -1;  // -1: none routed
+  int routed = 0;
+  bool thr_tuned = false;
+  std::vector<smp_ctx *> lanes;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
 };
 
 namespace {
 
 // Total scratch the rank slabs of one batch may take.
 constexpr size_t kSlabBudget = 24ull << 30;
+// Routed instances are dealt to this many single-instance pipelines.
+constexpr int kRouteLanes = 4;
+// Instances of at most this n are never routed: their pipeline is all launch
+// latency.
+constexpr int kRouteMinN = 1024;
 
 int subs_for_window(int window) {
   if (window <= 0) return 8;
@@ -125,6 +141,7 @@ int apply_shape(smp_batch &b, const Shape &sh) {
 // Tuned shapes, per device, largest n and batch size (powers of two).
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int>, Shape> g_tuned;
+std::map<std::tuple<int, int, int>, int> g_tuned_thr;
 
 // Runs the kernel over the sample table and returns its device time.
 float time_shape(smp_batch &b, const Shape &sh, BatchInstance *sample, const int32_t *order, int k) {
@@ -177,16 +194,134 @@ Shape autotune(smp_batch &b, Shape start, const smp_batch_cfg *cfg) {
   return best;
 }
 
-// The batched step: reset the queue, run the persistent kernel, copy the
-// table (statuses, proposals) back to pinned host memory.
+// An instance the batch routed to the single-instance pipeline: its status
+// and proposal count, from that pipeline's control block, into its table row
+// (one thread; enqueued after the pipeline on the same stream).
+__global__ void k_route_report(const Control *__restrict__ ctrl, BatchInstance *__restrict__ table, int idx) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int status = ctrl->status;
+  table[idx].status = status;
+  table[idx].proposals = status ? 0ull : ctrl->proposals;
+}
+
+// How many instances (largest first) have n above thr.
+int routed_count(const smp_batch &b, int thr) {
+  if (thr <= 0) return 0;
+  int r = 0;
+  while (r < b.count && b.inst[b.order[r]].n > thr) ++r;
+  return r;
+}
+
+// Routes the instances above thr (thr <= 0: none).  The lanes are created on
+// first use with every buffer a solve of the largest routed n takes, so that
+// a captured step allocates nothing.
+int set_threshold(smp_batch &b, int thr) {
+  Ctx &c = b.ctx->c;
+  b.threshold_n = thr > 0 ? thr : -1;
+  b.routed = routed_count(b, thr);
+  if (!b.routed) return SMP_OK;
+  if (!b.ev_fork && cudaEventCreateWithFlags(&b.ev_fork, cudaEventDisableTiming) != cudaSuccess)
+    return c.fail_cuda("route event");
+  while (static_cast<int>(b.lanes.size()) < kRouteLanes) {
+    smp_cfg lc = {};
+    lc.device = c.device;
+    smp_ctx *x = nullptr;
+    int rc = smp_b200_create(&x, &lc);
+    if (rc) return rc;
+    b.lanes.push_back(x);
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return c.fail_cuda("route event");
+    b.ev_join.push_back(e);
+  }
+  const int top = b.inst[b.order[0]].n;
+  for (smp_ctx *x : b.lanes) {
+    const int rc = reserve_buffers(x->c, top);
+    if (rc) {
+      c.last_error = x->c.last_error;
+      return rc;
+    }
+  }
+  return SMP_OK;
+}
+
+// The batched step: reset the queue; fork the routed instances to the lanes
+// (each solve followed by k_route_report into its table row); run the
+// persistent kernel on the rest; join; copy the table (statuses, proposals)
+// back to pinned host memory.
 int enqueue_step(smp_batch &b, cudaStream_t s) {
-  if (cudaMemsetAsync(b.d_queue.ptr, 0, sizeof(int), s) != cudaSuccess) return b.ctx->c.fail_cuda("queue reset");
-  int rc = launch_batch(b, s, b.grid, b.d_order.as<int32_t>(), b.count, 1);
+  Ctx &c = b.ctx->c;
+  if (cudaMemsetAsync(b.d_queue.ptr, 0, sizeof(int), s) != cudaSuccess) return c.fail_cuda("queue reset");
+  int rc = SMP_OK;
+  const int lanes = std::min(b.routed, static_cast<int>(b.lanes.size()));
+  if (lanes > 0) {
+    if (cudaEventRecord(b.ev_fork, s) != cudaSuccess) return c.fail_cuda("route fork");
+    for (int l = 0; l < lanes; ++l)
+      if (cudaStreamWaitEvent(b.lanes[l]->c.stream, b.ev_fork, 0) != cudaSuccess) return c.fail_cuda("route fork");
+    for (int k = 0; !rc && k < b.routed; ++k) {
+      Ctx &lc = b.lanes[k % lanes]->c;
+      const int i = b.order[k];
+      const smp_instance &in = b.inst[i];
+      rc = solve_enqueue(lc, in.pref_m, in.pref_w, in.n, in.match, SMP_F_DEVICE_PTRS);
+      if (!rc) {
+        k_route_report<<<1, 32, 0, lc.stream>>>(lc.d_ctrl.as<Control>(), b.d_table.as<BatchInstance>(), i);
+        rc = lc.check_launch("k_route_report");
+      }
+      if (rc) c.last_error = lc.last_error;
+    }
+  }
+  if (!rc && b.count > b.routed)
+    rc = launch_batch(b, s, std::min(b.grid, b.count - b.routed), b.d_order.as<int32_t>() + b.routed,
+                      b.count - b.routed, 1);
+  // join every lane, even after an error: a capture must end joined
+  for (int l = 0; l < lanes; ++l)
+    if ((cudaEventRecord(b.ev_join[l], b.lanes[l]->c.stream) != cudaSuccess ||
+         cudaStreamWaitEvent(s, b.ev_join[l], 0) != cudaSuccess) &&
+        !rc)
+      rc = c.fail_cuda("route join");
   if (rc) return rc;
   if (cudaMemcpyAsync(b.h_table, b.d_table.ptr, sizeof(smp_instance) * b.count, cudaMemcpyDeviceToHost, s) !=
       cudaSuccess)
-    return b.ctx->c.fail_cuda("table readback");
+    return c.fail_cuda("table readback");
   return SMP_OK;
+}
+
+// Device time of one uncaptured step (the best of two after a warm-up).
+float time_step(smp_batch &b) {
+  Ctx &c = b.ctx->c;
+  float best = 1e30f;
+  for (int rep = 0; rep < 3; ++rep) {
+    if (cudaEventRecord(b.ev0, c.stream) != cudaSuccess || enqueue_step(b, c.stream) != SMP_OK ||
+        cudaEventRecord(b.ev1, c.stream) != cudaSuccess || cudaStreamSynchronize(c.stream) != cudaSuccess) {
+      cudaGetLastError();
+      return 1e30f;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b.ev0, b.ev1);
+    if (rep > 0) best = std::min(best, ms);
+  }
+  return best;
+}
+
+// Routing none, or the largest 8, 32 or 128 instances (those above
+// kRouteMinN), each timed as a whole step; returns the fastest threshold.
+int tune_threshold(smp_batch &b) {
+  std::vector<int> cands = {-1};
+  for (int r : {8, 32, 128}) {
+    if (r >= b.count) break;
+    const int thr = std::max(b.inst[b.order[r]].n, kRouteMinN);  // at most r instances above it
+    if (routed_count(b, thr) > 0 && std::find(cands.begin(), cands.end(), thr) == cands.end()) cands.push_back(thr);
+  }
+  int best_thr = -1;
+  float best = 1e30f;
+  for (int thr : cands) {
+    if (set_threshold(b, thr)) continue;
+    const float ms = time_step(b);
+    if (ms < best) {
+      best = ms;
+      best_thr = thr;
+    }
+  }
+  return best_thr;
 }
 
 void fill_batch_stats(const smp_batch &b, smp_instance *results, smp_batch_stats *st, float ms, int launches) {
@@ -267,6 +402,7 @@ int smp_b200_batch_create(smp_ctx *ctx, const smp_instance *inst, int32_t count,
     }
     b->max_n = std::max(b->max_n, static_cast<int>(inst[i].n));
   }
+  b->inst.assign(inst, inst + count);
   // Work queue order: largest instances first (longest-processing-time).
   b->order.resize(count);
   std::iota(b->order.begin(), b->order.end(), 0);
@@ -283,6 +419,7 @@ int smp_b200_batch_create(smp_ctx *ctx, const smp_instance *inst, int32_t count,
   const bool want_tune = !(cfg && cfg->tune < 0) &&
                          !(cfg && cfg->block_threads > 0 && cfg->ctas_per_sm > 0 && cfg->window > 0 &&
                            cfg->rank_smem_kb != 0);
+  const bool want_thr = !(cfg && cfg->tune < 0) && !(cfg && cfg->threshold_n != 0);
   // Without tuning, shrink a default shape that does not fit (large max_n).
   while (!shape_fits(c, b->max_n, sh) && sh.rank_kb > 0) sh.rank_kb -= 32;
   if (!shape_fits(c, b->max_n, sh) && !(cfg && cfg->ctas_per_sm > 0)) sh.per_sm = 1;
@@ -348,6 +485,36 @@ int smp_b200_batch_create(smp_ctx *ctx, const smp_instance *inst, int32_t count,
     b->tuned = true;
   }
   rc = apply_shape(*b, sh);
+  if (rc) {
+    smp_b200_batch_destroy(b);
+    return rc;
+  }
+  // Routing to the all-SM pipeline: as configured, or timed on the batch.
+  int thr = cfg && cfg->threshold_n > 0 ? cfg->threshold_n : -1;
+  if (want_thr) {
+    const auto key = std::make_tuple(c.device, b->max_n, 31 - __builtin_clz(static_cast<unsigned>(count)));
+    bool cached = false;
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      auto it = g_tuned_thr.find(key);
+      if (it != g_tuned_thr.end()) {
+        thr = it->second;
+        cached = true;
+      }
+    }
+    if (!cached) {
+      thr = tune_threshold(*b);
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      g_tuned_thr[key] = thr;
+    }
+    b->thr_tuned = true;
+  }
+  rc = set_threshold(*b, thr);
+  // one uncaptured step first: kernel attributes are set outside the capture
+  if (!rc && b->routed) {
+    rc = enqueue_step(*b, c.stream);
+    if (!rc) rc = c.sync("routed step");
+  }
   if (rc) {
     smp_b200_batch_destroy(b);
     return rc;
@@ -426,6 +593,7 @@ int smp_b200_batch_config(const smp_batch *b, smp_batch_cfg *out) {
   out->use_graph = b->exec ? 1 : -1;
   out->rank_smem_kb = b->rank_kb > 0 ? b->rank_kb : -1;
   out->tune = b->tuned ? 1 : -1;
+  out->threshold_n = b->threshold_n;
   return SMP_OK;
 }
 
@@ -438,6 +606,9 @@ void smp_b200_batch_destroy(smp_batch *b) {
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->h_table) cudaFreeHost(b->h_table);
+    for (smp_ctx *x : b->lanes) smp_b200_destroy(x);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    for (cudaEvent_t e : b->ev_join) cudaEventDestroy(e);
     b->d_table.release();
     b->d_order.release();
     b->d_queue.release();

@@ -123,13 +123,9 @@ void plan(Ctx &c) {
 
 int enqueue_precheck(Ctx &c, bool allow_perfect) {
   const int n = c.n;
-  Control init = {};
-  init.free_count = n;
-  init.allow_perfect = allow_perfect ? 1 : 0;
-  init.allow_query = c.query_ok ? 1 : 0;
-  std::memcpy(c.h_ctrl, &init, sizeof(Control));
-  if (cudaMemcpyAsync(c.d_ctrl.ptr, c.h_ctrl, sizeof(Control), cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
-    return c.fail_cuda("control reset");
+  k_control_init<<<1, 128, 0, c.stream>>>(c.d_ctrl.as<Control>(), n, allow_perfect ? 1 : 0, c.query_ok ? 1 : 0);
+  c.launches++;
+  if (const int rc = c.check_launch("k_control_init")) return rc;
   const size_t words = (static_cast<size_t>(n) + 31) / 32;
   if (cudaMemsetAsync(c.d_seen.ptr, 0, words * 4, c.stream) != cudaSuccess) return c.fail_cuda("seen reset");
   const int grid = std::max(1, std::min(c.sm_count * 4, (n + 255) / 256));
@@ -1311,9 +1307,10 @@ int smp_b200_invert(smp_ctx *ctx, const int32_t *pref_w, int32_t n, int32_t *ran
     src = c.d_pref_w.as<int32_t>();
     dst = c.d_rank.as<int32_t>();
   }
-  std::memset(c.h_ctrl, 0, sizeof(Control));
-  if (cudaMemcpyAsync(c.d_ctrl.ptr, c.h_ctrl, sizeof(Control), cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
-    return c.fail_cuda("control reset");
+  k_control_init<<<1, 128, 0, c.stream>>>(c.d_ctrl.as<Control>(), 0, 0, 0);
+  c.launches++;
+  rc = c.check_launch("k_control_init");
+  if (rc) return rc;
   if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
   rc = enqueue_invert<int32_t>(c, src, dst, kGateAlways);
   if (rc) return rc;

@@ -87,6 +87,24 @@ __device__ __forceinline__ bool any_unset<int32_t>(uint4 v) {
 }
 
 // ---------------------------------------------------------------------------
+// A solve's control block, reset on the device: solves enqueued back to back
+// on one stream, or replayed from a captured graph, each start from their own
+// reset (a copy from a host staging buffer would read whatever an earlier
+// solve's readback left there by the time it ran).  One CTA.
+// ---------------------------------------------------------------------------
+__global__ void k_control_init(Control *__restrict__ ctrl, int n, int allow_perfect, int allow_query) {
+  static_assert(sizeof(Control) % 4 == 0, "control block of whole words");
+  int *words = reinterpret_cast<int *>(ctrl);
+  for (int i = threadIdx.x; i < static_cast<int>(sizeof(Control) / 4); i += blockDim.x) words[i] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ctrl->free_count = n;
+    ctrl->allow_perfect = allow_perfect;
+    ctrl->allow_query = allow_query;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Precheck.  Marks each man's first choice in an n-bit bitmap (seen, zeroed
 // by the host).  The last block to finish counts the distinct first choices
 // and decides: perfect (all distinct, if allowed) and the mode -- query mode

@@ -153,8 +153,11 @@ def test_autotuned_shape(ctx):
 def test_fixed_shape_is_kept(ctx):
     insts, meta = make_batch(ctx, 20, seed=23, n_lo=16, n_hi=500)
     with pb.Batch(ctx, insts, block_threads=256, ctas_per_sm=4, window=64, rank_smem_kb=-1) as batch:
-        assert batch.config() == {"block_threads": 256, "ctas_per_sm": 4, "window": 64, "use_graph": 1,
-                                  "rank_smem_kb": -1, "tune": -1}
+        cfg = batch.config()
+        thr = cfg.pop("threshold_n")
+        assert cfg == {"block_threads": 256, "ctas_per_sm": 4, "window": 64, "use_graph": 1,
+                       "rank_smem_kb": -1, "tune": -1}
+        assert thr == -1  # nothing above 1024 to route
         status, props, st = batch.run()
     assert st["failed"] == 0
 
@@ -179,3 +182,53 @@ def test_batch_top_of_the_mix_against_oracle(ctx):
     for (pm, pw, mt), p in zip(insts, props):
         want, wp = oracle.gs_seq(pm.cpu().numpy(), pw.cpu().numpy())
         assert np.array_equal(mt.cpu().numpy(), want) and p == wp
+
+
+# -- the largest instances routed to the all-SM pipeline -----------------------
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_routed_instances_match_the_oracle(ctx, use_graph):
+    # Instances above threshold_n run the single-instance pipeline on side
+    # streams beside the persistent kernel (forked and joined inside the
+    # captured graph); the rest run in the batch.  Every kind on both sides,
+    # and a defective instance among the routed ones, which alone fails.
+    import torch
+
+    sizes = [(pb.SMP_GEN_UNIFORM, 3000), (pb.SMP_GEN_CONGESTED, 2500), (pb.SMP_GEN_CORRELATED, 2100),
+             (pb.SMP_GEN_UNIFORM, 1800), (pb.SMP_GEN_CORRELATED, 1600), (pb.SMP_GEN_UNIFORM, 1400),
+             (pb.SMP_GEN_CONGESTED, 1200), (pb.SMP_GEN_UNIFORM, 900), (pb.SMP_GEN_CORRELATED, 300),
+             (pb.SMP_GEN_CONGESTED, 200), (pb.SMP_GEN_UNIFORM, 64)]
+    insts = []
+    for b, (kind, n) in enumerate(sizes):
+        pm, pw = ctx.generate(kind, n, seed=41, salt=b, param=KIND_PARAM[kind])
+        insts.append((pm, pw, torch.full((n,), -1, dtype=torch.int32, device=pm.device)))
+    bad = 5  # n = 1400: routed
+    insts[bad][1][7, 2] = insts[bad][1][7, 3]
+    with pb.Batch(ctx, insts, use_graph=use_graph, threshold_n=1300) as batch:
+        assert batch.config()["threshold_n"] == 1300
+        for _ in range(2):  # a replay gives the same answers
+            for _, _, mt in insts:
+                mt.fill_(-1)
+            status, props, st = batch.run()
+            assert status[bad] == pb.SMP_ERR_INVALID_INPUT and st["failed"] == 1
+            for i, ((pm, pw, mt), p) in enumerate(zip(insts, props)):
+                if i == bad:
+                    continue
+                assert status[i] == 0
+                want, wp = oracle.gs_seq(pm.cpu().numpy(), pw.cpu().numpy())
+                assert np.array_equal(mt.cpu().numpy(), want) and p == wp, i
+
+
+def test_autotuned_threshold_is_reported(ctx):
+    # A mix reaching n = 4096: the autotuner times routing none and the
+    # largest 8, 32 and 128 instances, and keeps the fastest; whichever it
+    # keeps, the answers equal the single solves'.
+    insts, meta = make_batch(ctx, 160, seed=43, n_lo=16, n_hi=4096)
+    with pb.Batch(ctx, insts) as batch:
+        thr = batch.config()["threshold_n"]
+        assert thr == -1 or thr >= 1024
+        status, props, st = batch.run()
+    assert st["failed"] == 0
+    for k in sorted(range(len(meta)), key=lambda k: -meta[k][0])[:12] + list(range(0, 160, 16)):
+        pm, pw, mt = insts[k]
+        want, wst = ctx.solve(pm, pw)
+        assert np.array_equal(mt.cpu().numpy(), want.cpu().numpy()) and props[k] == wst["proposals"]
