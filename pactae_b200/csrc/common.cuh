@@ -50,7 +50,7 @@ struct Control {
   int32_t coop_count;
   int32_t swap_next;      // k_swap_gs: next woman that has not proposed yet
   int32_t w_differ;       // k_swap_screen: a pref_w row differs from row 0
-  int32_t pad1;
+  int32_t swap_over;      // k_swap_gs: women stopped at the end of what the device holds of their rows
   int2 coop_chain[32];
 };
 

@@ -147,12 +147,9 @@ void HostLink::work(int t) {
   int used = 0;
   bool ok = true;
   std::string why;
-  for (int g = 0; g < total; ++g) {
-    int p, r0, r1;
-    group_rows(g, &p, &r0, &r1);
-    const Part &P = parts_[p];
-    const size_t e = static_cast<size_t>(r1) * n_;
-    for (size_t b = static_cast<size_t>(r0) * n_; b < e; b += kSlotEntries, ++piece) {
+  // entries [b, e) of the part's matrices, in pieces of at most one slot
+  const auto send = [&](const Part &P, size_t b, size_t e) {
+    for (; b < e; b += kSlotEntries, ++piece) {
       if (static_cast<int>(piece % workers_) != t || !ok) continue;
       const int slot = 2 * t + (used & 1);
       if (used >= 2 && cudaEventSynchronize(slot_ev_[slot]) != cudaSuccess) {
@@ -170,6 +167,19 @@ void HostLink::work(int t) {
         continue;
       }
       ++used;
+    }
+  };
+  for (int g = 0; g < total; ++g) {
+    int p, r0, r1;
+    group_rows(g, &p, &r0, &r1);
+    const Part &P = parts_[p];
+    if (P.row_ids) {
+      for (int i = r0; i < r1; ++i) {
+        const size_t b = static_cast<size_t>(P.row_ids[i]) * n_;
+        send(P, b, b + n_);
+      }
+    } else {
+      send(P, static_cast<size_t>(r0) * n_, static_cast<size_t>(r1) * n_);
     }
     if (ok && cudaEventRecord(group_ev_[static_cast<size_t>(t) * kMaxGroups + g], st) != cudaSuccess) {
       ok = false;

@@ -179,9 +179,10 @@ class HostLink {
   static constexpr size_t kSlotEntries = size_t{1} << 20;  // 2 MiB of uint16
   static constexpr int kMaxGroups = 32;
   struct Part {
-    const int32_t *src;  // host, rows x n
-    uint16_t *dst;       // device, rows x n
-    int rows;
+    const int32_t *src;  // host, n columns
+    uint16_t *dst;       // device, n columns
+    int rows;            // rows sent: 0 .. rows-1, or row_ids[0 .. rows-1]
+    const int32_t *row_ids = nullptr;  // host; rows to send, each a row of src and dst
   };
   HostLink() = default;
   HostLink(const HostLink &) = delete;
@@ -194,7 +195,7 @@ class HostLink {
   // row groups; group g of part p is global group p * groups + g.  The
   // copies are queued after the work already queued on `after`.
   int start(const Part *parts, int nparts, int n, int groups, cudaStream_t after);
-  // Rows [r0, r1) of global group g (row0 of that group's part).
+  // Rows [r0, r1) of global group g (indices into row_ids for a listed part).
   void group_rows(int g, int *part, int *r0, int *r1) const;
   // Blocks until every worker has queued its pieces of global group g, then
   // makes `stream` wait for them on the device.
@@ -262,6 +263,9 @@ struct Ctx {
   DeviceBuf d_pref_m, d_pref_w, d_rank, d_rankT, d_pr, d_prefix, d_bid, d_tailq, d_seen, d_ctrl, d_match;
   DeviceBuf d_pw16, d_pm16;  // pref_w and pref_m packed to uint16 (host-input solves)
   DeviceBuf d_swap_pos;  // women-proposing solves: position of each woman in the men's shared list
+  // host-input women-proposing solves: which women's rows are whole on the
+  // device, the women stopped at the end of theirs (two lists), row ids
+  DeviceBuf d_swap_full, d_swap_over, d_swap_rows;
   // Host-input solves: the host threads that pack and screen, and the link
   // that sends packed rows through them (created on first use).
   std::unique_ptr<HostPool> pack_pool;
@@ -276,10 +280,11 @@ struct Ctx {
   static constexpr int kCopyChunks = 16;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_chunk[kCopyChunks] = {};
-  std::array<DeviceBuf *, 23> buffers() {
+  std::array<DeviceBuf *, 26> buffers() {
     return {&d_pref_m, &d_pref_w, &d_pw16, &d_pm16, &d_rank,    &d_rankT,    &d_pr,     &d_prefix, &d_bid,    &d_tailq,
             &d_seen,   &d_ctrl,   &d_match,   &d_husband,  &d_prank,  &d_qcnt,   &d_qlist,
-            &gen_keys_a, &gen_keys_b, &gen_seg, &gen_temp, &gen_aux, &d_swap_pos};
+            &gen_keys_a, &gen_keys_b, &gen_seg, &gen_temp, &gen_aux, &d_swap_pos, &d_swap_full, &d_swap_over,
+            &d_swap_rows};
   }
   int launches = 0;  // kernels launched since the last stage / call
   smp_stats stats = {};

@@ -123,13 +123,14 @@ void plan(Ctx &c) {
 
 int enqueue_precheck(Ctx &c, bool allow_perfect) {
   const int n = c.n;
-  k_control_init<<<1, 128, 0, c.stream>>>(c.d_ctrl.as<Control>(), n, allow_perfect ? 1 : 0, c.query_ok ? 1 : 0);
-  c.launches++;
-  if (const int rc = c.check_launch("k_control_init")) return rc;
+  // zeroed on the device, never copied from the host block (k_precheck)
+  if (cudaMemsetAsync(c.d_ctrl.ptr, 0, sizeof(Control), c.stream) != cudaSuccess)
+    return c.fail_cuda("control reset");
   const size_t words = (static_cast<size_t>(n) + 31) / 32;
   if (cudaMemsetAsync(c.d_seen.ptr, 0, words * 4, c.stream) != cudaSuccess) return c.fail_cuda("seen reset");
   const int grid = std::max(1, std::min(c.sm_count * 4, (n + 255) / 256));
-  k_precheck<<<grid, 256, 0, c.stream>>>(c.pref_m, n, c.d_seen.as<uint32_t>(), c.d_ctrl.as<Control>());
+  k_precheck<<<grid, 256, 0, c.stream>>>(c.pref_m, n, c.d_seen.as<uint32_t>(), c.d_ctrl.as<Control>(),
+                                         allow_perfect ? 1 : 0, c.query_ok ? 1 : 0);
   c.launches++;
   return c.check_launch("k_precheck");
 }
@@ -798,7 +799,8 @@ int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped, boo
     if (cudaMemsetAsync(bid, 0xFF, sizeof(unsigned long long) * static_cast<size_t>(n), c.stream) != cudaSuccess)
       return c.fail_cuda("swap bid reset");
     if (cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
-    k_swap_gs<<<c.sm_count * 4, 256, 0, c.stream>>>(c.pref_m, c.pref_w, pos, bid, n, ctrl);
+    k_swap_gs<<<c.sm_count * 4, 256, 0, c.stream>>>(c.pref_m, c.pref_w, pos, bid, n, ctrl, nullptr, n, nullptr,
+                                                    nullptr, 0);
     c.launches++;
     rc = c.check_launch("k_swap_gs");
     if (!rc && cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
@@ -850,6 +852,18 @@ bool streamed_fits(const Ctx &c, uint32_t flags) {
          c.tail_threshold > 0 && c.n >= kStreamMinN;
 }
 
+// The context's host threads (created on first use): up to 16.  On a
+// 16-core host, 8, 12 and 16 packed and sent an n = 30000 list in the same
+// 37 ms, bound by reading it from host DRAM; comparing the men's rows with
+// row 0 took 58, 53 and 44 ms.
+HostPool *host_pool(Ctx &c) {
+  if (!c.pack_pool) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    c.pack_pool.reset(new (std::nothrow) HostPool(static_cast<int>(std::min(hw, 16u))));
+  }
+  return c.pack_pool.get();
+}
+
 // Host-input solves send their lists packed to uint16 -- half the bytes on
 // the host link, which is what a host-input solve of n = 30000 waits for --
 // through the context's HostLink, when the host has threads to pack with.
@@ -864,10 +878,7 @@ bool link_ready(Ctx &c, bool both) {
   const size_t bytes = sizeof(uint16_t) * static_cast<size_t>(n) * n;
   if (c.d_pw16.ensure(bytes)) return false;
   if (both && c.d_pm16.ensure(bytes)) return false;
-  // twelve threads: on a 16-core host, 8, 12 and 16 packed and sent an
-  // n = 30000 list in the same 37 ms, bound by reading it from host DRAM
-  if (!c.pack_pool) c.pack_pool.reset(new (std::nothrow) HostPool(static_cast<int>(std::min(hw, 12u))));
-  if (!c.pack_pool) return false;
+  if (!host_pool(c)) return false;
   if (!c.link) {
     c.link.reset(new (std::nothrow) HostLink());
     if (!c.link || c.link->open(c.pack_pool.get()) != SMP_OK) {
@@ -919,11 +930,7 @@ int send_packed(Ctx &c, const HostLink::Part *parts, int nparts, int groups, OnG
 // Does every row of the host matrix pref_m equal row 0?  Rows are compared
 // on the context's host threads, which stop at the first difference.
 bool host_rows_equal_row0(Ctx &c, const int32_t *pref_m, int n) {
-  if (!c.pack_pool) {
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    c.pack_pool.reset(new (std::nothrow) HostPool(static_cast<int>(std::min(hw, 12u))));
-    if (!c.pack_pool) return false;
-  }
+  if (!host_pool(c)) return false;
   std::atomic<bool> differ{false};
   const size_t row_bytes = sizeof(int32_t) * static_cast<size_t>(n);
   const auto job = [&](int i, int parts) {
@@ -935,6 +942,149 @@ bool host_rows_equal_row0(Ctx &c, const int32_t *pref_m, int n) {
   };
   c.pack_pool->run(job);
   return !differ.load();
+}
+
+// Host-input solve whose men all make the same first choice: perhaps one
+// list L for every man.  Then the stable matching is unique, the women
+// propose, and each woman reads her row only as far as the man she ends
+// with.  The k-th woman of L ends where the k-1 before her have not taken
+// her man, about n / (n - k + 1) entries in: only the last few hundred go
+// past a short prefix.
+//   1. Row 0 of pref_m and the first K entries of every woman's row cross
+//      as int32 while the host threads compare every man's row with row 0.
+//   2. A row differs: nothing more is sent here (shared = false); the caller
+//      runs the men's rank mode, which needs both lists.
+//   3. Else the kSharedDeepRows women L ranks lowest are sent whole through
+//      the link (packed, widened on the device), and the women propose.  A
+//      woman who reaches the end of what the device holds of her row stops;
+//      her row is sent and she resumes, until none stops.
+// Every entry sent is checked on the device: in range, and no man twice in
+// what was sent of a row.  Entries never sent are never read (as a
+// query-mode solve never reads a man's choices beyond his prefix).
+constexpr int kSharedDeepRows = 1024;
+
+int solve_shared_host(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, uint32_t flags, int32_t *match_out,
+                      bool &shared) {
+  const int n = c.n;
+  shared = false;
+  int32_t *dm = c.d_pref_m.as<int32_t>();
+  int32_t *dw = c.d_pref_w.as<int32_t>();
+  const size_t row = sizeof(int32_t) * static_cast<size_t>(n);
+  const int kw = std::min(n, c.K);
+  if (cudaMemcpyAsync(dm + c.K, pref_m + c.K, sizeof(int32_t) * (n - c.K), cudaMemcpyHostToDevice, c.stream) !=
+      cudaSuccess)
+    return c.fail_cuda("pref_m row 0 copy");
+  if (cudaMemcpy2DAsync(dw, row, pref_w, row, sizeof(int32_t) * kw, n, cudaMemcpyHostToDevice, c.stream) !=
+      cudaSuccess)
+    return c.fail_cuda("pref_w prefix copy");
+  if (!host_rows_equal_row0(c, pref_m, n)) return SMP_OK;
+  shared = true;
+  c.swapped = true;
+  int rc = c.d_swap_pos.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (!rc) rc = c.d_bid.ensure(sizeof(unsigned long long) * static_cast<size_t>(n));
+  if (!rc) rc = c.d_match.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (!rc) rc = c.d_swap_full.ensure(static_cast<size_t>(n));
+  if (!rc) rc = c.d_swap_over.ensure(2 * sizeof(int2) * static_cast<size_t>(n));
+  if (!rc) rc = c.d_swap_rows.ensure(sizeof(int32_t) * static_cast<size_t>(n));
+  if (rc) return rc;
+  Control *ctrl = c.d_ctrl.as<Control>();
+  int32_t *pos = c.d_swap_pos.as<int32_t>();
+  unsigned long long *bid = c.d_bid.as<unsigned long long>();
+  uint8_t *full = c.d_swap_full.as<uint8_t>();
+  int2 *over[2] = {c.d_swap_over.as<int2>(), c.d_swap_over.as<int2>() + n};
+  int32_t *d_rows = c.d_swap_rows.as<int32_t>();
+  const size_t check_smem = swap_screen_smem(n);
+  const int grid = std::max(1, std::min(c.sm_count * 4, (n + 255) / 256));
+  const int row_grid = std::max(1, std::min(c.sm_count * 8, n));
+
+  // Sends the listed women's rows whole (ids in [0, n)), widens them into
+  // dw, checks them and marks them whole.
+  const auto send_rows = [&](const std::vector<int32_t> &rows) -> int {
+    const int count = static_cast<int>(rows.size());
+    if (!count) return SMP_OK;
+    if (cudaMemcpyAsync(d_rows, rows.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, c.stream) !=
+        cudaSuccess)
+      return c.fail_cuda("row list copy");
+    HostLink::Part part = {pref_w, c.d_pw16.as<uint16_t>(), count, rows.data()};
+    int r = send_packed(c, &part, 1, 1, [&](int, int r0, int r1) {
+      k_widen16_rows<<<std::max(1, std::min(r1 - r0, c.sm_count * 4)), 256, 0, c.stream>>>(
+          c.d_pw16.as<uint16_t>(), dw, d_rows + r0, r1 - r0, n);
+      c.launches++;
+      return c.check_launch("k_widen16_rows");
+    });
+    if (r) return r;
+    k_swap_rows_check<<<std::max(1, std::min(count, c.sm_count * 8)), 256, check_smem, c.stream>>>(
+        dw, n, d_rows, count, n, ctrl);
+    k_swap_mark_full<<<std::max(1, std::min(c.sm_count, (count + 255) / 256)), 256, 0, c.stream>>>(full, d_rows,
+                                                                                                  count, n);
+    c.launches += 2;
+    return c.check_launch("k_swap_rows_check");
+  };
+  const auto reset_queue = [&]() -> int {  // swap_next, w_differ, swap_over
+    return cudaMemsetAsync(reinterpret_cast<char *>(ctrl) + offsetof(Control, swap_next), 0, 3 * sizeof(int32_t),
+                           c.stream) == cudaSuccess
+               ? SMP_OK
+               : c.fail_cuda("swap queue reset");
+  };
+
+  if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  if (cudaMemsetAsync(pos, 0xFF, sizeof(int32_t) * static_cast<size_t>(n), c.stream) != cudaSuccess ||
+      cudaMemsetAsync(full, 0, static_cast<size_t>(n), c.stream) != cudaSuccess ||
+      cudaMemsetAsync(bid, 0xFF, sizeof(unsigned long long) * static_cast<size_t>(n), c.stream) != cudaSuccess)
+    return c.fail_cuda("swap reset");
+  k_swap_pos<<<grid, 256, 0, c.stream>>>(dm, pos, n, ctrl);
+  k_swap_rows_check<<<row_grid, 256, check_smem, c.stream>>>(dw, n, nullptr, n, kw, ctrl);
+  c.launches += 2;
+  rc = c.check_launch("k_swap_rows_check");
+  // the women L ranks lowest go deepest: their rows whole from the start
+  std::vector<int32_t> rows;
+  rows.reserve(kSharedDeepRows);
+  for (int r = std::max(0, n - kSharedDeepRows); r < n; ++r)
+    if (static_cast<unsigned>(pref_m[r]) < static_cast<unsigned>(n)) rows.push_back(pref_m[r]);
+  if (!rc) rc = send_rows(rows);
+  if (!rc && cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = reset_queue();
+  if (rc) return rc;
+  k_swap_gs<<<c.sm_count * 4, 256, 0, c.stream>>>(dm, dw, pos, bid, n, ctrl, full, kw, over[0], nullptr, 0);
+  c.launches++;
+  rc = c.check_launch("k_swap_gs");
+  for (int round = 0; !rc; ++round) {
+    rc = read_control(c);
+    if (!rc) rc = c.sync("women's proposals");
+    if (rc || c.h_ctrl->status) break;
+    const int stopped = c.h_ctrl->swap_over;
+    if (stopped <= 0 || stopped > n) break;
+    std::vector<int2> list(stopped);
+    if (cudaMemcpy(list.data(), over[round & 1], sizeof(int2) * stopped, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      rc = c.fail_cuda("stopped women");
+      break;
+    }
+    rows.clear();
+    for (const int2 &e : list)
+      if (static_cast<unsigned>(e.x) < static_cast<unsigned>(n)) rows.push_back(e.x);
+    rc = send_rows(rows);
+    if (!rc) rc = reset_queue();
+    if (rc) break;
+    k_swap_gs<<<std::max(1, std::min(c.sm_count * 4, (stopped + 7) / 8)), 256, 0, c.stream>>>(
+        dm, dw, pos, bid, n, ctrl, full, kw, over[(round + 1) & 1], over[round & 1], stopped);
+    c.launches++;
+    rc = c.check_launch("k_swap_gs");
+  }
+  if (rc) return rc;
+  if (cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess ||
+      cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess)
+    return c.fail_cuda("event");
+  if (!c.h_ctrl->status) {
+    k_swap_match<<<grid, 256, 0, c.stream>>>(dm, bid, c.d_match.as<int32_t>(), n, ctrl);
+    c.launches++;
+    rc = c.check_launch("k_swap_match");
+    if (!rc) rc = copy_match_out(c, match_out, (flags & SMP_F_DEVICE_PTRS) != 0);
+  }
+  if (!rc && cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+  if (!rc) rc = read_control(c);
+  if (!rc) rc = c.sync("solve");
+  return rc;
 }
 
 int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
@@ -985,28 +1135,39 @@ int solve_streamed(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t
                             c.mode_cfg == 0 && swap_screen_smem(n) <= c.smem_optin;
     bool shared = false;
     if (!c.h_ctrl->perfect) {
-      if (!try_shared && link_ready(c, true)) {
-        // Both lists cross packed, pref_w first; each row group is widened
-        // back to int32 on the device as it lands.
-        const HostLink::Part parts[2] = {{pref_w, c.d_pw16.as<uint16_t>(), n}, {pref_m, c.d_pm16.as<uint16_t>(), n}};
-        rc = send_packed(c, parts, 2, kRankGroups, [&](int p, int r0, int r1) {
-          return enqueue_widen16(c, p ? c.d_pm16.as<uint16_t>() : c.d_pw16.as<uint16_t>(), p ? dm : dw,
-                                 static_cast<size_t>(r0) * n, static_cast<size_t>(r1) * n);
-        });
-      } else {
-        if (cudaMemcpyAsync(dw, pref_w, row * n, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
-          rc = c.fail_cuda("pref_w copy");
-        if (!rc && try_shared) {
-          if (cudaMemcpyAsync(dm + c.K, pref_m + c.K, sizeof(int32_t) * (n - c.K), cudaMemcpyHostToDevice,
-                              c.stream) != cudaSuccess)
-            rc = c.fail_cuda("pref_m row 0 copy");
-          if (!rc) shared = host_rows_equal_row0(c, pref_m, n);
+      bool screened = false;  // the men's rows were compared on the host already
+      if (try_shared && link_ready(c, false)) {
+        // completes the solve when the men share one list
+        rc = solve_shared_host(c, pref_m, pref_w, flags, match_out, shared);
+        screened = true;
+        swapped = !rc && shared;
+      }
+      if (!rc && !swapped) {
+        if ((!try_shared || screened) && link_ready(c, true)) {
+          // Both lists cross packed, pref_w first; each row group is widened
+          // back to int32 on the device as it lands.
+          const HostLink::Part parts[2] = {{pref_w, c.d_pw16.as<uint16_t>(), n},
+                                           {pref_m, c.d_pm16.as<uint16_t>(), n}};
+          rc = send_packed(c, parts, 2, kRankGroups, [&](int p, int r0, int r1) {
+            return enqueue_widen16(c, p ? c.d_pm16.as<uint16_t>() : c.d_pw16.as<uint16_t>(), p ? dm : dw,
+                                   static_cast<size_t>(r0) * n, static_cast<size_t>(r1) * n);
+          });
+        } else {
+          if (cudaMemcpyAsync(dw, pref_w, row * n, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+            rc = c.fail_cuda("pref_w copy");
+          if (!rc && try_shared && !screened) {
+            if (cudaMemcpyAsync(dm + c.K, pref_m + c.K, sizeof(int32_t) * (n - c.K), cudaMemcpyHostToDevice,
+                                c.stream) != cudaSuccess)
+              rc = c.fail_cuda("pref_m row 0 copy");
+            if (!rc) shared = host_rows_equal_row0(c, pref_m, n);
+          }
+          if (!rc && !shared) rc = copy_rest_of_m();
         }
-        if (!rc && !shared) rc = copy_rest_of_m();
       }
     }
-    if (!rc && cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
-    if (!rc && shared) rc = solve_swapped(c, flags, match_out, swapped, true);
+    if (!rc && !swapped && cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess)
+      rc = c.fail_cuda("event");
+    if (!rc && shared && !swapped) rc = solve_swapped(c, flags, match_out, swapped, true);
     if (!rc && !swapped) rc = enqueue_init(c);
     if (!rc && !swapped && cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
     if (!rc && !swapped) rc = enqueue_core(c);
@@ -1307,10 +1468,7 @@ int smp_b200_invert(smp_ctx *ctx, const int32_t *pref_w, int32_t n, int32_t *ran
     src = c.d_pref_w.as<int32_t>();
     dst = c.d_rank.as<int32_t>();
   }
-  k_control_init<<<1, 128, 0, c.stream>>>(c.d_ctrl.as<Control>(), 0, 0, 0);
-  c.launches++;
-  rc = c.check_launch("k_control_init");
-  if (rc) return rc;
+  if (cudaMemsetAsync(c.d_ctrl.ptr, 0, sizeof(Control), c.stream) != cudaSuccess) return c.fail_cuda("control reset");
   if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
   rc = enqueue_invert<int32_t>(c, src, dst, kGateAlways);
   if (rc) return rc;

@@ -87,33 +87,26 @@ __device__ __forceinline__ bool any_unset<int32_t>(uint4 v) {
 }
 
 // ---------------------------------------------------------------------------
-// A solve's control block, reset on the device: solves enqueued back to back
-// on one stream, or replayed from a captured graph, each start from their own
-// reset (a copy from a host staging buffer would read whatever an earlier
-// solve's readback left there by the time it ran).  One CTA.
-// ---------------------------------------------------------------------------
-__global__ void k_control_init(Control *__restrict__ ctrl, int n, int allow_perfect, int allow_query) {
-  static_assert(sizeof(Control) % 4 == 0, "control block of whole words");
-  int *words = reinterpret_cast<int *>(ctrl);
-  for (int i = threadIdx.x; i < static_cast<int>(sizeof(Control) / 4); i += blockDim.x) words[i] = 0;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    ctrl->free_count = n;
-    ctrl->allow_perfect = allow_perfect;
-    ctrl->allow_query = allow_query;
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Precheck.  Marks each man's first choice in an n-bit bitmap (seen, zeroed
 // by the host).  The last block to finish counts the distinct first choices
 // and decides: perfect (all distinct, if allowed) and the mode -- query mode
 // when at least a quarter of the first choices are distinct (proposals spread
 // over the women, so each man stays within his prefix), rank mode otherwise
 // (a few women draw most first proposals and men go deep into their lists).
+// The control block arrives zeroed by a memset on the same stream (a copy
+// from a host staging buffer would read whatever an earlier solve's readback
+// left there by the time it ran, when solves are queued back to back or
+// replayed from a graph); the switches come as arguments, and the precheck
+// writes them and the free count into it.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_precheck(const int32_t *__restrict__ pref_m, int n,
-                                                  uint32_t *__restrict__ seen, Control *ctrl) {
+                                                  uint32_t *__restrict__ seen, Control *ctrl, int allow_perfect,
+                                                  int allow_query) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctrl->free_count = n;
+    ctrl->allow_perfect = allow_perfect;
+    ctrl->allow_query = allow_query;
+  }
   const int stride = gridDim.x * blockDim.x;
   for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += stride) {
     const int w = __ldg(pref_m + static_cast<size_t>(m) * n);
@@ -142,8 +135,8 @@ __global__ void __launch_bounds__(256) k_precheck(const int32_t *__restrict__ pr
   if (threadIdx.x == 0) {
     const int distinct = s_count;
     ctrl->distinct = distinct;
-    ctrl->perfect = (ctrl->allow_perfect && distinct == n && ctrl->status == 0) ? 1 : 0;
-    ctrl->mode = (ctrl->allow_query && 4ll * distinct >= n) ? kModeQuery : kModeRank;
+    ctrl->perfect = (allow_perfect && distinct == n && ctrl->status == 0) ? 1 : 0;
+    ctrl->mode = (allow_query && 4ll * distinct >= n) ? kModeQuery : kModeRank;
   }
 }
 
@@ -825,12 +818,12 @@ __global__ void __launch_bounds__(256) k_qinvert_p16(const uint16_t *__restrict_
 // the packing makes of an entry outside [0, n) -- widens to 65535, still
 // >= n (n <= 65535 here), so the kernels that read the entry report it.
 // Eight entries per thread step: one 16-byte load and two 16-byte stores
-// where all eight lie inside the span, one by one at its ragged ends.
-__global__ void __launch_bounds__(256) k_widen16(const uint16_t *__restrict__ src, int32_t *__restrict__ dst,
-                                                 size_t begin, size_t end) {
+// where all eight lie inside the span, one by one at its ragged ends.  Thread
+// `first` of `stride` threads takes steps first, first + stride, ...
+__device__ __forceinline__ void widen_span(const uint16_t *__restrict__ src, int32_t *__restrict__ dst, size_t begin,
+                                           size_t end, size_t first, size_t stride) {
   const size_t base = begin & ~size_t{7};
-  const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x * 8;
-  for (size_t i = base + (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) * 8; i < end; i += stride) {
+  for (size_t i = base + first * 8; i < end; i += stride * 8) {
     if (i >= begin && i + 8 <= end) {
       const uint4 v = __ldcs(reinterpret_cast<const uint4 *>(src + i));
       const int4 lo = make_int4(static_cast<int>(v.x & 0xFFFFu), static_cast<int>(v.x >> 16),
@@ -844,6 +837,22 @@ __global__ void __launch_bounds__(256) k_widen16(const uint16_t *__restrict__ sr
       const size_t j1 = i + 8 < end ? i + 8 : end;
       for (size_t j = i < begin ? begin : i; j < j1; ++j) dst[j] = src[j];
     }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_widen16(const uint16_t *__restrict__ src, int32_t *__restrict__ dst,
+                                                 size_t begin, size_t end) {
+  widen_span(src, dst, begin, end, static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x,
+             static_cast<size_t>(gridDim.x) * blockDim.x);
+}
+
+// The same for the listed rows rows[0 .. count) (ids already checked to lie
+// in [0, n) on the host), one row per CTA at a time.
+__global__ void __launch_bounds__(256) k_widen16_rows(const uint16_t *__restrict__ src, int32_t *__restrict__ dst,
+                                                      const int32_t *__restrict__ rows, int count, int n) {
+  for (int i = blockIdx.x; i < count; i += gridDim.x) {
+    const size_t b = static_cast<size_t>(__ldg(rows + i)) * n;
+    widen_span(src, dst, b, b + n, threadIdx.x, blockDim.x);
   }
 }
 

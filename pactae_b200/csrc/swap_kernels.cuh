@@ -13,6 +13,9 @@
 //   k_swap_screen  every pref_m row equals row 0 (else swap_fail), and every
 //                  pref_w row is a permutation (else the invalid-input status)
 //   k_swap_gs      the women's proposals, one warp per chain
+//   k_swap_rows_check, k_swap_mark_full
+//                  host-input solves: the parts of pref_w sent, checked, and
+//                  which rows are whole
 //   k_swap_match   match[m] from the men's final bids; the men's proposal count
 //   k_swap_direct  women who share one list M as well: match[M[k]] = L[k]
 //                  (the k-th man of the women's list with the k-th woman of
@@ -142,14 +145,25 @@ __global__ void __launch_bounds__(256) k_swap_screen(const int32_t *__restrict__
 // displaced together with where she resumes.  Each warp carries one woman:
 // her next 32 men are read at once, the first man whose current word is
 // worse than hers takes her proposal, and a displaced woman continues in the
-// same warp.  A woman runs out of men only on input that is not a
-// permutation, which the screen has excluded; the bound keeps every read in
-// her row regardless.
+// same warp.
+//   Rows on the device: with full == nullptr every woman's whole row; else
+// woman w's whole row where full[w] is set and her first `depth` entries
+// otherwise (host-input solves send only those).  A woman who reaches the
+// end of what the device holds of her row stops and is appended to `over`
+// as (w, position), to resume once her row has been sent (start/start_count
+// then list the women this launch resumes, instead of women 0..n-1 from
+// position 0).  Gale-Shapley's result does not depend on that order.  An
+// entry out of range is reported; a woman who runs out of her whole row
+// (input that is not a permutation) too.
 __global__ void __launch_bounds__(256) k_swap_gs(const int32_t *__restrict__ pref_m,
                                                  const int32_t *__restrict__ pref_w,
                                                  const int32_t *__restrict__ pos,
-                                                 unsigned long long *__restrict__ bid, int n, Control *ctrl) {
+                                                 unsigned long long *__restrict__ bid, int n, Control *ctrl,
+                                                 const uint8_t *__restrict__ full, int depth,
+                                                 int2 *__restrict__ over, const int2 *__restrict__ start,
+                                                 int start_count) {
   const int lane = threadIdx.x & 31;
+  const int total = start ? start_count : n;
   int w = -1, r0 = 0;
   uint32_t key = 0;
   for (;;) {
@@ -157,23 +171,44 @@ __global__ void __launch_bounds__(256) k_swap_gs(const int32_t *__restrict__ pre
       int i = 0;
       if (lane == 0) i = atomicAdd(&ctrl->swap_next, 1);
       i = __shfl_sync(kFullMask, i, 0);
-      if (i >= n) break;
-      w = i;
-      r0 = 0;
+      if (i >= total) break;
+      if (start) {
+        const int2 e = start[i];
+        w = e.x;
+        r0 = e.y;
+      } else {
+        w = i;
+        r0 = 0;
+      }
       key = static_cast<uint32_t>(__ldg(pos + w));
     }
-    if (r0 >= n) {
-      if (lane == 0) report(ctrl, kStatusInvalidInput, w);
+    const int lim = (full == nullptr || full[w]) ? n : depth;  // entries of her row on the device
+    if (r0 >= lim) {
+      if (lane == 0) {
+        if (lim >= n) {
+          report(ctrl, kStatusInvalidInput, w);
+        } else {
+          const int k = atomicAdd(&ctrl->swap_over, 1);
+          over[k] = make_int2(w, r0);
+        }
+      }
       w = -1;
       continue;
     }
     const int r = r0 + lane;
-    const int m = r < n ? __ldg(pref_w + static_cast<size_t>(w) * n + r) : 0;
-    const bool open = r < n && static_cast<unsigned>(m) < static_cast<unsigned>(n) &&
-                      static_cast<uint32_t>(ld_relaxed_u64(bid + m) >> 32) > key;
+    const bool in_row = r < lim;
+    const int m = in_row ? __ldg(pref_w + static_cast<size_t>(w) * n + r) : 0;
+    const bool valid = static_cast<unsigned>(m) < static_cast<unsigned>(n);
+    const bool open = in_row && valid && static_cast<uint32_t>(ld_relaxed_u64(bid + m) >> 32) > key;
     const unsigned hit = __ballot_sync(kFullMask, open);
+    const unsigned bad = __ballot_sync(kFullMask, in_row && !valid);
+    if (bad) {  // an entry out of range
+      if (lane == __ffs(bad) - 1) report(ctrl, kStatusInvalidInput, m);
+      w = -1;
+      continue;
+    }
     if (!hit) {
-      r0 += 32;
+      r0 = min(r0 + 32, lim);
       continue;
     }
     const int f = __ffs(hit) - 1;
@@ -192,6 +227,54 @@ __global__ void __launch_bounds__(256) k_swap_gs(const int32_t *__restrict__ pre
     key = static_cast<uint32_t>(old >> 32);
     w = __ldg(pref_m + key);
     r0 = static_cast<int>(old & 0xFFFFFFFFull) + 1;
+  }
+}
+
+// Host-input shared-list solves: checks the entries of pref_w the device
+// holds -- the first `cols` of every row (rows == nullptr: rows 0..count-1)
+// or of the listed rows -- are in range and name no man twice.  One row per
+// CTA at a time, n bits of shared memory.
+__global__ void __launch_bounds__(256) k_swap_rows_check(const int32_t *__restrict__ pref_w, int n,
+                                                         const int32_t *__restrict__ rows, int count, int cols,
+                                                         Control *ctrl) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t *seen = reinterpret_cast<uint32_t *>(smem_raw);
+  const int words = (n + 31) >> 5;
+  bool bad = false;
+  int bad_value = 0;
+  for (int i = blockIdx.x; i < count; i += gridDim.x) {
+    const int w = rows ? __ldg(rows + i) : i;
+    for (int k = threadIdx.x; k < words; k += blockDim.x) seen[k] = 0u;
+    __syncthreads();
+    if (static_cast<unsigned>(w) < static_cast<unsigned>(n)) {
+      const int32_t *row = pref_w + static_cast<size_t>(w) * n;
+      for (int r = threadIdx.x; r < cols; r += blockDim.x) {
+        const int v = __ldg(row + r);
+        if (static_cast<unsigned>(v) >= static_cast<unsigned>(n)) {
+          bad = true;
+          bad_value = v;
+          continue;
+        }
+        const uint32_t bit = 1u << (v & 31);
+        if (atomicOr(seen + (v >> 5), bit) & bit) {
+          bad = true;
+          bad_value = v;
+        }
+      }
+    } else if (threadIdx.x == 0) {
+      bad = true;
+      bad_value = w;
+    }
+    __syncthreads();  // the bitmap is cleared for the next row only after this one
+  }
+  if (bad) report(ctrl, kStatusInvalidInput, bad_value);
+}
+
+// full[rows[i]] = 1 for the rows now whole on the device.
+__global__ void k_swap_mark_full(uint8_t *__restrict__ full, const int32_t *__restrict__ rows, int count, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const int w = __ldg(rows + i);
+    if (static_cast<unsigned>(w) < static_cast<unsigned>(n)) full[w] = 1;
   }
 }
 

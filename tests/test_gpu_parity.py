@@ -488,6 +488,62 @@ def test_host_input_men_sharing_one_list(case):
     assert st["mode"] == (0 if case == "twisted" else 3)
 
 
+@pytest.mark.parametrize("prefix_k", [1, 8, 0])
+@pytest.mark.parametrize("kind", [pb.SMP_GEN_CONGESTED, pb.SMP_GEN_REF_CONGESTED])
+def test_host_input_shared_list_sends_what_the_women_read(kind, prefix_k):
+    # Men sharing one list, host inputs: only row 0 of pref_m, every woman's
+    # first K entries and the 1024 women the shared list ranks lowest cross
+    # whole; a woman who reaches the end of what the device holds of her row
+    # stops, her row is sent and she resumes.  With K = 1 or 8 most women
+    # stop at least once (several rounds); with the default K none should.
+    n = 4099
+    pm, pw = oracle.generate(kind, n, 27)
+    want, props = oracle.gs_seq(pm, pw)
+    with pb.Context(prefix_k=prefix_k) as c:
+        for _ in range(2):  # the context's buffers are reused
+            match, st = c.solve(pm, pw)
+            assert np.array_equal(match, want) and st["proposals"] == props and st["mode"] == 3
+
+
+@pytest.mark.parametrize("where", ["deep_row", "prefix", "resumed_row"])
+def test_host_input_shared_list_checks_what_it_sends(where):
+    # Every entry sent is checked on the device.  A duplicate in the whole
+    # row of the woman the shared list ranks last, in the first K entries of
+    # a woman's row, or deep in the row of a woman who stops at the end of
+    # her first 8 entries and is sent whole: each is reported.
+    n = 4099
+    pm, pw = oracle.generate(pb.SMP_GEN_CONGESTED, n, 31)
+    pm, pw = pm.copy(), pw.copy()
+    shared = pm[0]
+    prefix_k = 0
+    if where == "deep_row":
+        w = int(shared[n - 1])
+        pw[w, n - 5] = pw[w, n - 4]
+    elif where == "prefix":
+        w = int(shared[5])
+        pw[w, 2] = pw[w, 3]
+    else:
+        # a woman outside the lowest 1024 of the shared list whose final man
+        # lies past her first 8 entries: she stops there and is sent whole
+        prefix_k = 8
+        want, _ = oracle.gs_seq(pm, pw)
+        husband = np.empty(n, np.int64)
+        husband[want] = np.arange(n)
+        rank_in_l = np.empty(n, np.int64)
+        rank_in_l[shared] = np.arange(n)
+        depth = np.array([int(np.nonzero(pw[v] == husband[v])[0][0]) for v in range(n)])
+        w = int(np.nonzero((depth > 8) & (depth < n - 3) & (rank_in_l < n - 1024))[0][0])
+        pw[w, n - 3] = pw[w, n - 2]
+    with pb.Context(prefix_k=prefix_k) as c:
+        with pytest.raises(pb.SmpError) as e:
+            c.solve(pm, pw)
+        assert e.value.status == pb.SMP_ERR_INVALID_INPUT
+        good_pm, good_pw = oracle.generate(pb.SMP_GEN_CONGESTED, n, 31)
+        match, st = c.solve(good_pm, good_pw)
+    want, props = oracle.gs_seq(good_pm, good_pw)
+    assert np.array_equal(match, want) and st["proposals"] == props
+
+
 @pytest.mark.parametrize("defect", ["none", "duplicate", "negative", "wraps_to_valid", "men_wrap"])
 def test_host_input_rank_mode_sends_packed_lists(defect):
     # Rank-mode host-input solves send both lists packed to 16 bits, in row
