@@ -582,9 +582,13 @@ def run_serving(ctx, args, dist: Dist) -> dict:
     checked = [0]
     rng = np.random.default_rng(6)
 
-    def one_load(srv, rate, count):
-        picks = rng.integers(0, pool_size, count)
-        outs = [torch.empty(pool[i][2], dtype=torch.int32, device=dev) for i in picks]
+    def one_load(srv, rate, count, pool, host=False):
+        # pool entries: (pref_m, pref_w, n, the matching solved alone)
+        picks = rng.integers(0, len(pool), count)
+        if host:
+            outs = [np.empty(pool[i][2], dtype=np.int32) for i in picks]
+        else:
+            outs = [torch.empty(pool[i][2], dtype=torch.int32, device=dev) for i in picks]
         gaps = rng.exponential(1.0 / rate, count) if rate else np.zeros(count)
         tickets = [None] * count
         results = [None] * count
@@ -610,27 +614,57 @@ def run_serving(ctx, args, dist: Dist) -> dict:
         lat = np.array([r["latency_ms"] for r in results])
         assert all(r["status"] == 0 for r in results)
         for k, i in enumerate(picks):
-            assert torch.equal(outs[k], solo[i]), f"served request {k} differs from its instance solved alone"
+            same = np.array_equal(outs[k], pool[i][3]) if host else torch.equal(outs[k], pool[i][3])
+            assert same, f"served request {k} differs from its instance solved alone"
         checked[0] += count
         return {"offered_per_s": round(rate, 1) if rate else None, "requests": count,
                 "solves_per_s": round(count / wall, 1), "p50_ms": round(float(np.percentile(lat, 50)), 3),
                 "p99_ms": round(float(np.percentile(lat, 99)), 3), "mean_n": int(np.mean([pool[i][2] for i in picks]))}
 
+    pool = [(pm, pw, n, m) for (pm, pw, n), m in zip(pool, solo)]
     with pb.Server() as srv:
-        one_load(srv, 0, 32)  # warm-up
-        sat = one_load(srv, 0, args.serving_requests)
+        one_load(srv, 0, 32, pool)  # warm-up
+        sat = one_load(srv, 0, args.serving_requests, pool)
         saturation = sat["solves_per_s"]
         loads = []
         for f in [float(x) for x in args.serving_loads.split(",") if x]:
-            r = one_load(srv, f * saturation, args.serving_requests)
+            r = one_load(srv, f * saturation, args.serving_requests, pool)
             r["load"] = f
             loads.append(r)
         st = srv.stats()
-    return {"workload": "Poisson stream of single instances, n log-uniform in [64, 16384] (seed 6), "
-                        "uniform/congested/correlated, pool of 48 instances resident in HBM, "
-                        "64 GiB admission budget", "saturation_solves_per_s": saturation,
-            "burst": sat, "loads": loads, "waves": st["waves"], "large_path": st["large"],
-            "peak_admitted_gb": round(st["peak_bytes"] / 1e9, 2), "matchings_checked": checked[0]}
+    out = {"workload": "Poisson stream of single instances, n log-uniform in [64, 16384] (seed 6), "
+                       "uniform/congested/correlated, pool of 48 instances resident in HBM, "
+                       "64 GiB admission budget", "saturation_solves_per_s": saturation,
+           "burst": sat, "loads": loads, "waves": st["waves"], "large_path": st["large"],
+           "peak_admitted_gb": round(st["peak_bytes"] / 1e9, 2)}
+    del pool, solo
+    # Host inputs: each request's lists are copied in when it is admitted
+    # (10 n^2 bytes held while it runs) and its matching copied back; a
+    # 4 GiB budget makes admission wait for room.
+    hpool = []
+    for b in range(16):
+        n, kind = pb.batch_instance(7, b, 64, 16384)
+        pm, pw = ctx.generate(kind, n, seed=7, salt=b, param=KIND_PARAM[kind])
+        hpm = torch.empty((n, n), dtype=torch.int32, pin_memory=True)
+        hpw = torch.empty((n, n), dtype=torch.int32, pin_memory=True)
+        hpm.copy_(pm)
+        hpw.copy_(pw)
+        hpool.append((hpm.numpy(), hpw.numpy(), n, ctx.solve(pm, pw)[0].cpu().numpy()))
+        del pm, pw
+    budget = 4 << 30
+    with pb.Server(hbm_budget=budget) as srv:
+        one_load(srv, 0, 8, hpool, host=True)  # warm-up
+        hsat = one_load(srv, 0, 64, hpool, host=True)
+        hhalf = one_load(srv, 0.5 * hsat["solves_per_s"], 64, hpool, host=True)
+        hhalf["load"] = 0.5
+        hst = srv.stats()
+    out["host_inputs"] = {"workload": "16 pinned host instances, n log-uniform in [64, 16384] (seed 7), "
+                                      "lists copied in on admission, matching copied back",
+                          "hbm_budget_gib": budget >> 30, "burst": hsat, "half_load": hhalf,
+                          "peak_admitted_gb": round(hst["peak_bytes"] / 1e9, 2),
+                          "mean_h2d_bytes_per_request": int(np.mean([8 * h[2] ** 2 for h in hpool]))}
+    out["matchings_checked"] = checked[0]
+    return out
 
 
 def config_roofline(n: int, st: dict, ms: float) -> dict:
