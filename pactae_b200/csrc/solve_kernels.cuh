@@ -1424,22 +1424,25 @@ __global__ void __launch_bounds__(1024, 1) k_tail_q(const int32_t *__restrict__ 
   uint32_t raw = 0;
   unsigned long long settled = 0;
   unsigned int hops = 0;
-  for (;;) {
-    if (m < 0) {
-      int i = 0;
-      if (lane == 0) i = atomicAdd(&s_next, 1);
-      i = __shfl_sync(kFullMask, i, 0);
-      if (i >= total) break;
-      if (i < queued) {
-        const int2 e = tail_queue[i];
-        m = e.x;
-        pos = e.y;
-      } else {
-        m = first_unstarted + (i - queued);
-        pos = 0;
-      }
-      raw = prefix_word(prefix, K, Kn, m, pos + lane);
+  // The warp's next man from the queue (false when none is left); called
+  // before the loop and where a chain ends, not at the top of every step.
+  const auto next_man = [&]() {
+    int i = 0;
+    if (lane == 0) i = atomicAdd(&s_next, 1);
+    i = __shfl_sync(kFullMask, i, 0);
+    if (i >= total) return false;
+    if (i < queued) {
+      const int2 e = tail_queue[i];
+      m = e.x;
+      pos = e.y;
+    } else {
+      m = first_unstarted + (i - queued);
+      pos = 0;
     }
+    raw = prefix_word(prefix, K, Kn, m, pos + lane);
+    return true;
+  };
+  for (bool more = next_man(); more;) {
     const int aborted = *reinterpret_cast<volatile int *>(&s_abort);  // tested at the end of the step
     const int r = pos + lane;
     const bool ok = r < Kn && raw != 0xFFFFFFFFu;
@@ -1488,6 +1491,16 @@ __global__ void __launch_bounds__(1024, 1) k_tail_q(const int32_t *__restrict__ 
       old = atom_min_relaxed_shared(sbid + w, (rk << 16) | static_cast<uint32_t>(m));
     }
     old = __shfl_sync(kFullMask, old, j);
+    // The common step -- accepted, displacing the holder whose window is
+    // already loading -- takes one branch; everything else the other side.
+    if (old == hw && (old >> 16) > rkj && hw != 0xFFFFFFFFu && !aborted) {
+      settled += j + 1;
+      hops++;
+      m = hm;
+      pos = hpos;
+      raw = next_raw;
+      continue;
+    }
     if ((old >> 16) <= rkj) {  // someone better got there first: read the bids again
       if (aborted) break;
       continue;
@@ -1495,7 +1508,9 @@ __global__ void __launch_bounds__(1024, 1) k_tail_q(const int32_t *__restrict__ 
     settled += j + 1;
     hops++;
     if (old == 0xFFFFFFFFu) {
-      m = -1;
+      if (aborted) break;
+      more = next_man();  // the chain ended at a free woman
+      continue;
     } else if (old == hw) {
       m = hm;
       pos = hpos;
