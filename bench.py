@@ -59,7 +59,9 @@ def parse_args():
     ap.add_argument("--bamboo-study", action="store_true",
                     help="the reference's GPU engine SmpEngineBamboo beside ours on the same B200 and instances")
     ap.add_argument("--bamboo-cases", default="0:2000:1,0:30000:2",
-                    help="kind:n:seed triples for --bamboo-study")
+                    help="kind:n:seed[:param] cases for --bamboo-study (param: the generator's, e.g. the "
+                         "group size of kind 5); the reference's Figure 9 matrix at n = 30000 is "
+                         "4:30000:9,3:30000:9,5:30000:9:5,6:30000:9")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 8192-instance batched leg")
@@ -939,15 +941,17 @@ def bamboo_cases(ctx, cases) -> list[dict]:
         return 0
 
     records = []
-    for kind, n, seed in cases:
+    for case in cases:
+        kind, n, seed = case[:3]
+        param = case[3] if len(case) > 3 else 0
         # host bytes at peak: our pinned lists (8 n^2), the engine's SmpObj and
         # its construction copies (16 n^2) and its host PR matrix (8 n^2)
         need = 32 * n * n
         if mem_available() < 2 * need:
-            records.append({"bamboo_study": f"kind {kind} n={n} seed {seed}", "unavailable":
+            records.append({"bamboo_study": f"kind {kind} n={n} seed {seed} param {param}", "unavailable":
                             f"host memory: {mem_available() >> 30} GiB available, {2 * need >> 30} GiB wanted"})
             continue
-        dpm, dpw = ctx.generate(kind, n, seed)
+        dpm, dpw = ctx.generate(kind, n, seed, param=param)
         ours_match, _ = ctx.solve(dpm, dpw)  # warm-up
         dev_ms = []
         for _ in range(3):
@@ -992,7 +996,8 @@ def bamboo_cases(ctx, cases) -> list[dict]:
                         "engine_total_ms_first_run": round(sum(runs[0][1][:3]), 3)}
         best_dev = min(r["engine_total_ms"] for r in ref.values())
         best_e2e = min(r["end_to_end_ms"] for r in ref.values())
-        records.append({"bamboo_study": f"kind {kind} n={n} seed {seed}", "n": n, "kind": kind, "seed": seed,
+        records.append({"bamboo_study": f"kind {kind} n={n} seed {seed} param {param}", "n": n, "kind": kind,
+                        "seed": seed, "param": param,
                         "reference_smp_engine_bamboo": ref,
                         "ours": {"device_input_ms": round(min(dev_ms), 3), "host_input_e2e_ms": round(min(e2e_ms), 2)},
                         "speedup_vs_best_reference": {
