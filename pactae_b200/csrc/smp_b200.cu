@@ -927,12 +927,13 @@ int send_packed(Ctx &c, const HostLink::Part *parts, int nparts, int groups, OnG
   return rc;
 }
 
-// Does every row of the host matrix pref_m equal row 0?  Rows are compared
-// on the context's host threads, which stop at the first difference.
-bool host_rows_equal_row0(Ctx &c, const int32_t *pref_m, int n) {
+// Does every row of the host matrix pref_m equal row 0 (in its first `cols`
+// entries; all of them by default)?  Rows are compared on the context's host
+// threads, which stop at the first difference.
+bool host_rows_equal_row0(Ctx &c, const int32_t *pref_m, int n, int cols = -1) {
   if (!host_pool(c)) return false;
   std::atomic<bool> differ{false};
-  const size_t row_bytes = sizeof(int32_t) * static_cast<size_t>(n);
+  const size_t row_bytes = sizeof(int32_t) * static_cast<size_t>(cols < 0 ? n : cols);
   const auto job = [&](int i, int parts) {
     const int r0 = 1 + static_cast<int>(static_cast<int64_t>(n - 1) * i / parts);
     const int r1 = 1 + static_cast<int>(static_cast<int64_t>(n - 1) * (i + 1) / parts);
@@ -954,7 +955,10 @@ bool host_rows_equal_row0(Ctx &c, const int32_t *pref_m, int n) {
 //      as int32 while the host threads compare every man's row with row 0.
 //   2. A row differs: nothing more is sent here (shared = false); the caller
 //      runs the men's rank mode, which needs both lists.
-//   3. Else the kSharedDeepRows women L ranks lowest are sent whole through
+//   3. If every woman's row equals row 0 too (her first K entries first,
+//      then the whole row, on the host threads), only row 0 of pref_w is
+//      sent and the k-th man of that list pairs with the k-th woman of L.
+//   4. Else the kSharedDeepRows women L ranks lowest are sent whole through
 //      the link (packed, widened on the device), and the women propose.  A
 //      woman who reaches the end of what the device holds of her row stops;
 //      her row is sent and she resumes, until none stops.
@@ -1028,6 +1032,39 @@ int solve_shared_host(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, uint
   };
 
   if (cudaEventRecord(c.ev[kEvPrecheckEnd], c.stream) != cudaSuccess) return c.fail_cuda("event");
+  // The women may share one list M as well (their first K entries first,
+  // then every row on the host threads): the k-th man of M and the k-th
+  // woman of L then pair up, no proposals.  Only row 0 of pref_w is sent;
+  // it and L are checked before the pairing writes match[].
+  if (host_rows_equal_row0(c, pref_w, n, kw) && host_rows_equal_row0(c, pref_w, n)) {
+    if (cudaMemcpyAsync(dw + kw, pref_w + kw, sizeof(int32_t) * (n - kw), cudaMemcpyHostToDevice, c.stream) !=
+            cudaSuccess ||
+        cudaMemsetAsync(pos, 0xFF, sizeof(int32_t) * static_cast<size_t>(n), c.stream) != cudaSuccess ||
+        cudaMemsetAsync(d_rows, 0, sizeof(int32_t), c.stream) != cudaSuccess)  // the row list {0}
+      return c.fail_cuda("shared lists copy");
+    k_swap_pos<<<grid, 256, 0, c.stream>>>(dm, pos, n, ctrl);
+    k_swap_rows_check<<<1, 256, check_smem, c.stream>>>(dw, n, d_rows, 1, n, ctrl);
+    c.launches += 2;
+    rc = c.check_launch("k_swap_rows_check");
+    if (!rc) rc = read_control(c);
+    if (!rc) rc = c.sync("shared lists check");
+    if (rc) return rc;
+    if (!c.h_ctrl->status) {
+      if (cudaEventRecord(c.ev[kEvInvertEnd], c.stream) != cudaSuccess ||
+          cudaEventRecord(c.ev[kEvInitEnd], c.stream) != cudaSuccess ||
+          cudaEventRecord(c.ev[kEvBulkEnd], c.stream) != cudaSuccess ||
+          cudaEventRecord(c.ev[kEvCoreEnd], c.stream) != cudaSuccess)
+        return c.fail_cuda("event");
+      k_swap_direct<<<grid, 256, 0, c.stream>>>(dm, dw, c.d_match.as<int32_t>(), n, ctrl);
+      c.launches++;
+      rc = c.check_launch("k_swap_direct");
+      if (!rc) rc = copy_match_out(c, match_out, (flags & SMP_F_DEVICE_PTRS) != 0);
+      if (!rc && cudaEventRecord(c.ev[kEvPostEnd], c.stream) != cudaSuccess) rc = c.fail_cuda("event");
+      if (!rc) rc = read_control(c);
+      if (!rc) rc = c.sync("solve");
+    }
+    return rc;
+  }
   if (cudaMemsetAsync(pos, 0xFF, sizeof(int32_t) * static_cast<size_t>(n), c.stream) != cudaSuccess ||
       cudaMemsetAsync(full, 0, static_cast<size_t>(n), c.stream) != cudaSuccess ||
       cudaMemsetAsync(bid, 0xFF, sizeof(unsigned long long) * static_cast<size_t>(n), c.stream) != cudaSuccess)

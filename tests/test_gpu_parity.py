@@ -505,18 +505,21 @@ def test_host_input_shared_list_sends_what_the_women_read(kind, prefix_k):
             assert np.array_equal(match, want) and st["proposals"] == props and st["mode"] == 3
 
 
-@pytest.mark.parametrize("where", ["deep_row", "prefix", "resumed_row"])
+@pytest.mark.parametrize("where", ["deep_row", "prefix", "resumed_row", "both_shared_row0"])
 def test_host_input_shared_list_checks_what_it_sends(where):
     # Every entry sent is checked on the device.  A duplicate in the whole
     # row of the woman the shared list ranks last, in the first K entries of
     # a woman's row, or deep in the row of a woman who stops at the end of
     # her first 8 entries and is sent whole: each is reported.
     n = 4099
-    pm, pw = oracle.generate(pb.SMP_GEN_CONGESTED, n, 31)
+    kind = pb.SMP_GEN_REF_CONGESTED if where == "both_shared_row0" else pb.SMP_GEN_CONGESTED
+    pm, pw = oracle.generate(kind, n, 31)
     pm, pw = pm.copy(), pw.copy()
     shared = pm[0]
     prefix_k = 0
-    if where == "deep_row":
+    if where == "both_shared_row0":
+        pw[:, n - 9] = pw[:, n - 8]  # every woman's row alike, none a permutation: only row 0 is sent
+    elif where == "deep_row":
         w = int(shared[n - 1])
         pw[w, n - 5] = pw[w, n - 4]
     elif where == "prefix":
@@ -538,7 +541,7 @@ def test_host_input_shared_list_checks_what_it_sends(where):
         with pytest.raises(pb.SmpError) as e:
             c.solve(pm, pw)
         assert e.value.status == pb.SMP_ERR_INVALID_INPUT
-        good_pm, good_pw = oracle.generate(pb.SMP_GEN_CONGESTED, n, 31)
+        good_pm, good_pw = oracle.generate(kind, n, 31)
         match, st = c.solve(good_pm, good_pw)
     want, props = oracle.gs_seq(good_pm, good_pw)
     assert np.array_equal(match, want) and st["proposals"] == props
