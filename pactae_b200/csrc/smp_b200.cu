@@ -685,7 +685,13 @@ int solve_swapped(Ctx &c, uint32_t flags, int32_t *match_out, bool &swapped, boo
 int solve_staged(Ctx &c, const int32_t *pref_m, const int32_t *pref_w, int32_t n, int32_t *match_out,
                  uint32_t flags, smp_stats *st) {
   // the checker, a disabled tail or a configured tail window (whose tail
-  // kernel serves either mode) take the fully gated pipeline
+  // kernel serves either mode) take the fully gated pipeline.  The tail is
+  // this n's (plan), not the previous solve's: a fresh context's first solve
+  // would otherwise always take the gated pipeline.
+  if (n > 0 && n <= SMP_B200_MAX_N) {
+    c.n = n;
+    plan(c);
+  }
   if ((flags & SMP_F_CHECK) || !(c.tail_threshold > 0) || c.tail_window_cfg > 0) {
     int rc = solve_enqueue(c, pref_m, pref_w, n, match_out, flags);
     if (!rc) rc = c.sync("solve");

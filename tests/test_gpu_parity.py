@@ -347,6 +347,19 @@ def test_men_sharing_one_list_women_propose(ctx, kind, n, device):
     assert np.array_equal(match2, want2) and st2["proposals"] == props2 and st2["mode"] != 3
 
 
+def test_first_solve_of_a_fresh_context_takes_the_shared_list_path():
+    # The dispatch reads the plan of the n being solved, so a fresh
+    # context's first solve (no earlier plan) takes the women-proposing pass
+    # for men sharing a list, as every later solve does.
+    for kind in (pb.SMP_GEN_REF_CONGESTED, pb.SMP_GEN_CONGESTED):
+        with pb.Context() as c:
+            pm, pw = c.generate(kind, 3001, seed=19)
+            match, st = c.solve(pm, pw)
+            assert st["mode"] == 3 and st["proposals"] == 3001 * 3002 // 2
+            want, _ = oracle.gs_seq(to_host(pm), to_host(pw))
+            assert np.array_equal(to_host(match), want)
+
+
 def test_bad_arguments(ctx):
     with pytest.raises(pb.SmpError) as e:
         ctx.generate(pb.SMP_GEN_SOLO, 2, seed=1)
