@@ -188,8 +188,13 @@ __global__ void __launch_bounds__(256) k_swap_gs(const int32_t *__restrict__ pre
         if (lim >= n) {
           report(ctrl, kStatusInvalidInput, w);
         } else {
+          // at most n: a woman who stops holds no man, so nothing sends her
+          // back into this launch
           const int k = atomicAdd(&ctrl->swap_over, 1);
-          over[k] = make_int2(w, r0);
+          if (k < n)
+            over[k] = make_int2(w, r0);
+          else
+            report(ctrl, kStatusInvalidInput, w);
         }
       }
       w = -1;
